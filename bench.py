@@ -1,0 +1,415 @@
+"""Benchmark of the finite-difference path on B200.
+
+Headline workload: band-batched complex Laplace apply (GPAW kinetic operator,
+scale = -0.5, nn = 3: the 19-point 6th-order stencil) on 512 complex128 bands
+of a 96^3 fully periodic grid, h = 0.18 A, Bloch phases for k = (0.25, 0, 0),
+Re/Im ~ N(0, 1).  One step = one apply over all bands.  The metric is the
+algorithmic HBM bandwidth, 32 bytes per point (one complex128 read, one
+written), in GB/s.  The 7.25 GB input is far larger than the 126 MB L2, so no
+flush is needed between steps.
+
+The same JSON line carries, for the dominant kernel, the roofline against the
+measured copy bandwidth (MEASURED_PEAKS.json), the end-to-end figure through
+the public API with host buffers, the CPU baseline, the clocks seen during
+the timed region, and the Poisson solves/s (128^3 zero-boundary grid, 64
+Gaussians, eps = 2e-10) of the plain FP64 and the mixed-precision solver.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU: one process per GPU under torch.distributed.run; every rank applies
+the operator to its own 512 bands (weak scaling, no collective on the data
+path); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BOHR = 0.52917721092
+N = 96
+NBANDS = 512
+BYTES_PER_POINT = 32  # complex128 in + out
+K_VEC = (0.25, 0.0, 0.0)
+METRIC = 'stencil HBM GB/s (band-batched complex128 Laplace nn=3)'
+
+
+def workload_config(nbands=NBANDS):
+    return {'workload': 'complex128 Laplace nn=3, %d bands x %d^3 periodic, h=0.18 A, '
+                        'k=(0.25,0,0)' % (nbands, N),
+            'bands': nbands, 'grid': [N, N, N], 'nn': 3, 'dtype': 'complex128',
+            'bytes_per_point': BYTES_PER_POINT,
+            'l2_policy': 'inputs (7.25 GB) larger than L2 (126 MB); no flush needed'}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the headline kernel from the committed ncu
+    summary (profiles/star_kernel_c128_96.txt: a line 'traffic_bytes_per_launch: X')."""
+    path = os.path.join(ROOT, 'profiles', 'star_kernel_c128_96.txt')
+    try:
+        for line in open(path):
+            if line.startswith('traffic_bytes_per_launch:'):
+                return float(line.split(':', 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region (NVML).
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    REASONS = {0x4: 'sw_power_cap', 0x8: 'hw_slowdown', 0x20: 'sw_thermal_slowdown',
+               0x40: 'hw_thermal_slowdown', 0x80: 'hw_power_brake_slowdown'}
+
+    def __init__(self, period=0.02):
+        self.period = period
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.handle = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = self._handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.handle = None
+
+    def _handle(self):
+        import torch
+        pynvml = self.nvml
+        try:
+            props = torch.cuda.get_device_properties(torch.cuda.current_device())
+            bus = '%08x:%02x:%02x.0' % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            vis = os.environ.get('CUDA_VISIBLE_DEVICES', '0').split(',')[0]
+            return pynvml.nvmlDeviceGetHandleByIndex(int(vis) if vis.isdigit() else 0)
+
+    def _sample(self):
+        p = self.nvml
+        try:
+            self.samples.append(p.nvmlDeviceGetClockInfo(self.handle, p.NVML_CLOCK_SM))
+            mask = p.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+            for bit, name in self.REASONS.items():
+                if mask & bit:
+                    self.reasons.add(name)
+        except Exception:
+            pass
+
+    def _run(self):
+        while not self._stop.is_set():
+            self._sample()
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.handle is not None:
+            self._sample()
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.handle is not None:
+            self._stop.set()
+            self.thread.join()
+            self._sample()
+
+    def result(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': self.max_mhz, 'reasons': ['unavailable']}
+        return {'sm_mhz': float(np.median(self.samples)), 'sm_max_mhz': self.max_mhz,
+                'reasons': sorted(self.reasons), 'samples': len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# Distributed plumbing (one process per GPU).
+# ---------------------------------------------------------------------------
+def dist_setup(ngpus):
+    import torch
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device('cuda', local))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm.
+# ---------------------------------------------------------------------------
+class CpuStencil:
+    """The reference CPU path (oracle/_ref when it was built, else the oracle
+    port) applying the workload's operator to a sample of its bands with all
+    host threads."""
+
+    def __init__(self, nbands_sample, impl='ref'):
+        from oracle import geometry as G
+        from oracle import kernels as K
+        self.K = K
+        self.impl = impl if (impl != 'ref' or K.have_ref()) else 'port'
+        self.kind = 'reference' if self.impl == 'ref' else 'port'
+        gd = G.Grid((N,) * 3, (N * 0.18 / BOHR,) * 3, 1)
+        self.pbc = gd.pbc_c
+        self.c, self.o = G.laplace_stencil(gd, -0.5, 3)
+        rng = np.random.default_rng(2)
+        shape = (nbands_sample,) + tuple(gd.n_c)
+        self.a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        self.ph = G.bloch_phases(gd, K_VEC)
+        self.threads = os.cpu_count() or 1
+        self.nbands = nbands_sample
+        self.bytes = BYTES_PER_POINT * nbands_sample * N ** 3
+
+    def step(self):
+        self.K.fd_apply(self.c, self.o, self.pbc, self.a, self.ph, nthreads=self.threads,
+                        impl=self.impl)
+
+    def rate(self, min_seconds):
+        self.step()
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            self.step()
+            reps += 1
+            dt = time.perf_counter() - t0
+            if dt >= min_seconds:
+                return self.bytes * reps / dt / 1e9, reps, dt
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return 0
+    cpu = CpuStencil(16)
+    for _ in range(args.warmup):
+        cpu.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu.step()
+    total = time.perf_counter() - t0
+    value = float(args.steps * cpu.bytes / total / 1e9)
+    sample = '%d of the %d bands per step (%s C path, %d threads)' % (
+        cpu.nbands, NBANDS, cpu.kind, cpu.threads)
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'GB/s',
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': total / args.steps * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'complex128', 'data': 'synthetic',
+            'config': workload_config(),
+            'cpu_baseline': {'value': value, 'unit': 'GB/s', 'cores': cpu.threads,
+                             'kind': cpu.kind, 'sample': sample},
+            'e2e': {'value': value, 'unit': 'GB/s', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Poisson solves/s (128^3 zero boundary, 64 Gaussians, eps = 2e-10).
+# ---------------------------------------------------------------------------
+def poisson_rho(gd, ng, seed):
+    from math import pi
+    rng = np.random.default_rng(seed)
+    r = gd.get_grid_point_coordinates()
+    L = gd.cell_cv.diagonal()
+    q = np.array([1.0] * (ng // 2) + [-1.0] * (ng // 2))
+    rng.shuffle(q)
+    rho = np.zeros(tuple(gd.n_c))
+    for i in range(ng):
+        s = rng.uniform(0.4, 1.2) / BOHR
+        R = rng.uniform(2 / BOHR, L - 2 / BOHR)
+        d2 = sum((r[c] - R[c]) ** 2 for c in range(3))
+        rho += q[i] * (2 * pi * s * s) ** -1.5 * np.exp(-d2 / (2 * s * s))
+    return rho - rho.mean()
+
+
+def poisson_bench(nsolves=8):
+    import torch
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.poisson import PoissonSolver
+    Np = 128
+    gd = GridDescriptor((Np,) * 3, (Np * 0.2 / BOHR,) * 3, 0)
+    rho_h = poisson_rho(gd, 64, 3)
+    rho = torch.from_numpy(rho_h).cuda()
+    out = {'workload': '128^3 zero boundary, h=0.2 A, 64 Gaussians, nn=3, Jacobi, eps=2e-10'}
+    phis = {}
+    for prec in ('fp64', 'mixed'):
+        ps = PoissonSolver(3, 'J', 2e-10, precision=prec)
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        phi = torch.zeros_like(rho)
+        ps.solve(phi, rho)  # warm-up
+        lat = []
+        for _ in range(nsolves):
+            phi.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            niter = ps.solve(phi, rho)
+            torch.cuda.synchronize()
+            lat.append(time.perf_counter() - t0)
+        phis[prec] = phi.cpu().numpy()
+        lat = np.array(lat)
+        out[prec] = {'solves_per_s': float(1.0 / lat.mean()), 'p50_ms': float(np.median(lat) * 1e3),
+                     'p99_ms': float(np.percentile(lat, 99) * 1e3), 'vcycles': int(niter),
+                     'residual': float(ps.error)}
+    out['mixed_vs_fp64_speedup'] = out['mixed']['solves_per_s'] / out['fp64']['solves_per_s']
+    out['mixed_max_abs_vs_fp64'] = float(np.abs(phis['mixed'] - phis['fp64']).max())
+    return out, phis, rho_h, gd
+
+
+# ---------------------------------------------------------------------------
+# GPU arm.
+# ---------------------------------------------------------------------------
+def run_gpu_arm(args):
+    import torch
+    rank, world = dist_setup(args.gpus)
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.grid_descriptor import GridDescriptor
+
+    gd = GridDescriptor((N,) * 3, (N * 0.18 / BOHR,) * 3, 1)
+    lap = Laplace(gd, -0.5, 3, complex)
+    phase = np.exp(2j * np.pi * gd.sdisp_cd * np.array(K_VEC)[:, None])
+    g = torch.Generator(device='cuda')
+    g.manual_seed(2 + rank)
+    shape = (NBANDS,) + tuple(int(x) for x in gd.n_c)
+    a = torch.complex(torch.randn(shape, dtype=torch.float64, device='cuda', generator=g),
+                      torch.randn(shape, dtype=torch.float64, device='cuda', generator=g))
+    b = torch.empty_like(a)
+    stream = torch.cuda.current_stream()
+    nbytes = BYTES_PER_POINT * NBANDS * N ** 3
+
+    for _ in range(args.warmup):
+        lap.apply(a, b, phase)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler() as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            lap.apply(a, b, phase)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = max_over_ranks(ms, world)
+    value = world * nbytes / (ms_max * 1e-3) / 1e9
+    kernel_gbs = nbytes / (ms * 1e-3) / 1e9
+
+    # End to end through the public API with host buffers: pinned H2D copy of
+    # the bands, apply, D2H copy of the result, every step.
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    host_in = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+    host_in.copy_(a)
+    host_out = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        a.copy_(host_in, non_blocking=True)
+        lap.apply(a, b, phase)
+        host_out.copy_(b, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world)
+    e2e_value = world * nbytes / (e2e_ms * 1e-3) / 1e9
+    del host_in, host_out
+
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic()
+    line = {'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_max,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'complex128', 'data': 'synthetic (seeded N(0,1) bands)',
+            'config': dict(workload_config(), parallelism='bands sharded, %d per GPU' % NBANDS),
+            'roofline': {'bound': 'hbm', 'achieved': kernel_gbs, 'peak': peak, 'unit': 'GB/s',
+                         'frac': kernel_gbs / peak, 'peak_kind': peak_kind,
+                         'traffic': traffic, 'algorithmic_bytes_per_launch': nbytes,
+                         'kernel': 'star_kernel<cplx<double>,R=3>'},
+            'e2e': {'value': e2e_value, 'unit': 'GB/s', 'steps': e2e_steps,
+                    'h2d_bytes_per_step': nbytes // 2, 'd2h_bytes_per_step': nbytes // 2},
+            'gpu_launches': args.steps,
+            'clocks': clocks.result()}
+    if rank == 0 and world == 1 and not args.no_poisson:
+        try:
+            pb, _, _, _ = poisson_bench()
+            line['poisson'] = pb
+        except Exception as e:  # reported, never hidden
+            line['poisson'] = {'error': repr(e)}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = CpuStencil(16)
+        r, reps, dt = cpu.rate(args.cpu_seconds)
+        line['cpu_baseline'] = {'value': r, 'unit': 'GB/s', 'cores': cpu.threads,
+                                'kind': cpu.kind,
+                                'sample': '16 of the 512 bands, %d passes in %.1f s'
+                                          % (reps, dt)}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--e2e-steps', type=int, default=3)
+    ap.add_argument('--cpu-seconds', type=float, default=10.0)
+    ap.add_argument('--no-poisson', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,156 @@
+// capi.cu -- error reporting, device queries, reductions and small streaming
+// launches of libgpawfd.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "common.cuh"
+#include "internal.h"
+#include "util.cuh"
+
+namespace gfd {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return GFD_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return set_error(GFD_ENOMEM, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+  return set_error(GFD_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int check_launch(const char* what) { return check_cuda(cudaGetLastError(), what); }
+
+int num_sms() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cache[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
+int reduce_launch(int dtype, const void* a, int64_t n, bool square, double scale,
+                  double* partials, double* result, cudaStream_t s) {
+  if (dtype == GFD_FLOAT64) {
+    if (square)
+      partial_sum_kernel<double, true><<<kRedBlocks, kRedThreads, 0, s>>>(
+          static_cast<const double*>(a), n, partials);
+    else
+      partial_sum_kernel<double, false><<<kRedBlocks, kRedThreads, 0, s>>>(
+          static_cast<const double*>(a), n, partials);
+  } else if (dtype == GFD_FLOAT32) {
+    if (square)
+      partial_sum_kernel<float, true><<<kRedBlocks, kRedThreads, 0, s>>>(
+          static_cast<const float*>(a), n, partials);
+    else
+      partial_sum_kernel<float, false><<<kRedBlocks, kRedThreads, 0, s>>>(
+          static_cast<const float*>(a), n, partials);
+  } else {
+    return set_error(GFD_EINVAL, "reductions need a real dtype");
+  }
+  final_sum_kernel<<<1, kRedThreads, 0, s>>>(partials, kRedBlocks, scale, result);
+  return check_launch("partial_sum_kernel");
+}
+
+int final_sum_launch(const double* partials, int n, double scale, double* result,
+                     cudaStream_t s) {
+  final_sum_kernel<<<1, kRedThreads, 0, s>>>(partials, n, scale, result);
+  return check_launch("final_sum_kernel");
+}
+
+int axpby_launch(int ydtype, void* y, int xdtype, const void* x, double a, double b, int64_t n,
+                 cudaStream_t s) {
+  const int blocks = grid_for(n);
+  if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT64)
+    axpby_kernel<double, double><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+                                                        static_cast<const double*>(x), a, b, n);
+  else if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT32)
+    axpby_kernel<double, float><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+                                                       static_cast<const float*>(x), a, b, n);
+  else if (ydtype == GFD_FLOAT32 && xdtype == GFD_FLOAT32)
+    axpby_kernel<float, float><<<blocks, 256, 0, s>>>(static_cast<float*>(y),
+                                                      static_cast<const float*>(x), a, b, n);
+  else
+    return set_error(GFD_EINVAL, "axpby: unsupported dtype pair");
+  return check_launch("axpby_kernel");
+}
+
+int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cudaStream_t s) {
+  const int blocks = grid_for(n);
+  if (dtype == GFD_FLOAT64)
+    sub_const_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+                                                    static_cast<const double*>(x), c, n);
+  else if (dtype == GFD_FLOAT32)
+    sub_const_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(y),
+                                                   static_cast<const float*>(x), c, n);
+  else
+    return set_error(GFD_EINVAL, "sub_const: unsupported dtype");
+  return check_launch("sub_const_kernel");
+}
+
+int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s) {
+  const int blocks = grid_for(n);
+  if (ydtype == GFD_FLOAT32 && xdtype == GFD_FLOAT64)
+    convert_kernel<float, double><<<blocks, 256, 0, s>>>(static_cast<float*>(y),
+                                                         static_cast<const double*>(x), n);
+  else if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT32)
+    convert_kernel<double, float><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+                                                         static_cast<const float*>(x), n);
+  else
+    return set_error(GFD_EINVAL, "convert: unsupported dtype pair");
+  return check_launch("convert_kernel");
+}
+
+}  // namespace gfd
+
+using namespace gfd;
+
+extern "C" size_t gfd_last_error(char* buf, size_t len) {
+  const std::string& m = g_last_error;
+  if (buf && len > 0) {
+    size_t n = m.size() < len - 1 ? m.size() : len - 1;
+    std::memcpy(buf, m.data(), n);
+    buf[n] = '\0';
+  }
+  return m.size();
+}
+
+extern "C" const char* gfd_version(void) { return "gpaw-fd-b200 0.1 sm_100a"; }
+
+extern "C" int gfd_grid_sum(const double* a, int64_t n, double scale, double* result,
+                            void* stream) {
+  if (!result) return set_error(GFD_EINVAL, "null result pointer");
+  if (n < 0) return set_error(GFD_EINVAL, "negative size");
+  if (n == 0) {
+    *result = 0.0;
+    return GFD_OK;
+  }
+  if (!a) return set_error(GFD_EINVAL, "null array pointer");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* buf = nullptr;
+  int st = check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&buf),
+                                      sizeof(double) * (kRedBlocks + 1), s),
+                      "cudaMallocAsync(reduction)");
+  if (st) return st;
+  st = reduce_launch(GFD_FLOAT64, a, n, false, scale, buf, buf + kRedBlocks, s);
+  if (!st)
+    st = check_cuda(cudaMemcpyAsync(result, buf + kRedBlocks, sizeof(double),
+                                    cudaMemcpyDeviceToHost, s),
+                    "cudaMemcpyAsync(sum)");
+  cudaFreeAsync(buf, s);
+  if (!st) st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize(sum)");
+  return st;
+}

@@ -1,0 +1,80 @@
+// internal.h -- handle layouts and launchers shared by the C-ABI entry points
+// of libgpawfd (host code only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "gpaw_fd.h"
+
+struct gfd_operator {
+  int ncoefs = 0;
+  std::vector<double> coefs;
+  std::vector<int> off;  // ncoefs x 3
+  int n[3] = {0, 0, 0};
+  int mp = 0;            // halo width (largest |offset| component)
+  int per[3] = {0, 0, 0};
+  int real = 1;
+  int cfd = 1;
+  // Axis-aligned decomposition (star stencils).
+  bool star = false;
+  int R = 0;
+  double c0 = 0.0;
+  double cx[13] = {0}, cy[13] = {0}, cz[13] = {0};  // index 6 + k
+  double diag = 0.0;     // weight of the zero offset
+  // Device scratch of one grid for relaxation (Jacobi ping-pong / frozen
+  // copy for periodic Gauss-Seidel), allocated on first use.
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  int device = -1;
+};
+
+struct gfd_transformer {
+  int nin[3] = {0, 0, 0};
+  int nout[3] = {0, 0, 0};
+  int k = 2, nn = 1;
+  int pad[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  int skip[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  int per[3] = {0, 0, 0};
+  int real = 1;
+  int interpolate = 0;
+};
+
+namespace gfd {
+
+enum { OP_APPLY = 0, OP_JACOBI = 1, OP_RESIDUAL = 2 };
+
+int num_sms();
+
+// Stencil launch.  mode OP_APPLY: out = L in.  OP_JACOBI: out = Jacobi update
+// of in with source rho and weight w.  OP_RESIDUAL: out = L in - rho and, if
+// partials != nullptr, one sum of squares per CTA into partials.
+// in/out/rho point to nin bands.  phase_cd: 12 doubles (host) or nullptr.
+int op_launch(const gfd_operator* op, int dtype, int mode, const void* in, void* out,
+              const void* rho, int64_t nin, const double* phase_cd, double w,
+              double* partials, cudaStream_t s);
+// Number of partial sums op_launch(OP_RESIDUAL) writes for nin bands.
+int64_t op_partials(const gfd_operator* op, int dtype, int mode, int64_t nin);
+
+// Multicolour Gauss-Seidel sweeps (real).  frozen: scratch of one grid.
+int op_gs_sweeps(const gfd_operator* op, int dtype, void* phi, const void* rho, int nsweeps,
+                 void* frozen, cudaStream_t s);
+int op_gs_colors(const gfd_operator* op);
+
+int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,
+              const double* phases, cudaStream_t s);
+
+// Deterministic sum of n elements (float64 or float32 by dtype), SQUARE for
+// the sum of squares; result (device) = scale * sum.  partials needs
+// kRedBlocks doubles.
+int reduce_launch(int dtype, const void* a, int64_t n, bool square, double scale,
+                  double* partials, double* result, cudaStream_t s);
+int final_sum_launch(const double* partials, int n, double scale, double* result,
+                     cudaStream_t s);
+int axpby_launch(int ydtype, void* y, int xdtype, const void* x, double a, double b, int64_t n,
+                 cudaStream_t s);
+int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cudaStream_t s);
+int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s);
+
+}  // namespace gfd

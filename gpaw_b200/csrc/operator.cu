@@ -1,0 +1,238 @@
+// operator.cu -- gfd_operator_*: the _gpaw.Operator replacement
+// (c/operators.c:465-498 constructor, :316-405 apply, :49-91 relax,
+// :408-421 get_diagonal_element).
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "common.cuh"
+#include "internal.h"
+#include "stencil_launch.cuh"
+
+GFD_DECLARE_STENCIL_ENTRY(f64)
+GFD_DECLARE_STENCIL_ENTRY(f32)
+GFD_DECLARE_STENCIL_ENTRY(c128)
+GFD_DECLARE_STENCIL_ENTRY(c64)
+
+namespace gfd {
+
+static int check_dtype(const gfd_operator* op, int dtype) {
+  if (dtype < GFD_FLOAT64 || dtype > GFD_COMPLEX64)
+    return set_error(GFD_EINVAL, "unknown dtype " + std::to_string(dtype));
+  if (op->real != !dtype_is_complex(dtype))
+    return set_error(GFD_EINVAL, op->real ? "operator was built for real arrays"
+                                          : "operator was built for complex arrays");
+  return GFD_OK;
+}
+
+int op_launch(const gfd_operator* op, int dtype, int mode, const void* in, void* out,
+              const void* rho, int64_t nin, const double* phase_cd, double w,
+              double* partials, cudaStream_t s) {
+  if (nin <= 0) return GFD_OK;
+  const bool star = op->star;
+  switch (dtype) {
+    case GFD_FLOAT64:
+      return star ? star_f64(op, mode, in, out, rho, nin, phase_cd, w, partials, s)
+                  : general_f64(op, mode, in, out, rho, nin, phase_cd, w, partials, s);
+    case GFD_FLOAT32:
+      return star ? star_f32(op, mode, in, out, rho, nin, phase_cd, w, partials, s)
+                  : general_f32(op, mode, in, out, rho, nin, phase_cd, w, partials, s);
+    case GFD_COMPLEX128:
+      return star ? star_c128(op, mode, in, out, rho, nin, phase_cd, w, partials, s)
+                  : general_c128(op, mode, in, out, rho, nin, phase_cd, w, partials, s);
+    case GFD_COMPLEX64:
+      return star ? star_c64(op, mode, in, out, rho, nin, phase_cd, w, partials, s)
+                  : general_c64(op, mode, in, out, rho, nin, phase_cd, w, partials, s);
+  }
+  return set_error(GFD_EINVAL, "unknown dtype");
+}
+
+int64_t op_partials(const gfd_operator* op, int /*dtype*/, int /*mode*/, int64_t nin) {
+  return partials_count(op, nin);
+}
+
+// Smallest colour count for which no nonzero offset keeps the colour
+// (i0 + i1 + i2) mod ncolor; 0 if none up to 2*mp + 2.
+int op_gs_colors(const gfd_operator* op) {
+  for (int nc = 2; nc <= 2 * op->mp + 2; nc++) {
+    bool ok = true;
+    for (int c = 1; c < op->ncoefs && ok; c++) {
+      int s = op->off[3 * c] + op->off[3 * c + 1] + op->off[3 * c + 2];
+      if (((s % nc) + nc) % nc == 0) ok = false;
+    }
+    if (ok) return nc;
+  }
+  return 0;
+}
+
+int op_gs_sweeps(const gfd_operator* op, int dtype, void* phi, const void* rho, int nsweeps,
+                 void* frozen, cudaStream_t s) {
+  int nc = op_gs_colors(op);
+  if (nc == 0) return set_error(GFD_EUNSUPPORTED, "no valid colouring for this stencil");
+  if (dtype == GFD_FLOAT64)
+    return gs_typed<double>(op, static_cast<double*>(phi), static_cast<const double*>(rho),
+                            nsweeps, static_cast<double*>(frozen), nc, s);
+  if (dtype == GFD_FLOAT32)
+    return gs_typed<float>(op, static_cast<float*>(phi), static_cast<const float*>(rho), nsweeps,
+                           static_cast<float*>(frozen), nc, s);
+  return set_error(GFD_EINVAL, "relaxation needs a real dtype");
+}
+
+static int ensure_scratch(gfd_operator* op, size_t bytes) {
+  if (op->scratch && op->scratch_bytes >= bytes) return GFD_OK;
+  if (op->scratch) {
+    cudaFree(op->scratch);
+    op->scratch = nullptr;
+    op->scratch_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&op->scratch, bytes);
+  if (e != cudaSuccess) {
+    op->scratch = nullptr;
+    cudaGetLastError();
+    return set_error(GFD_ENOMEM, "cudaMalloc of relaxation scratch failed");
+  }
+  op->scratch_bytes = bytes;
+  cudaGetDevice(&op->device);
+  return GFD_OK;
+}
+
+}  // namespace gfd
+
+using namespace gfd;
+
+extern "C" int gfd_operator_create(int ncoefs, const double* coefs, const int64_t* offsets,
+                                   const int64_t size[3], int range, const int64_t neighbors[6],
+                                   int real, int cfd, gfd_operator** out) {
+  if (!out) return set_error(GFD_EINVAL, "null output handle");
+  *out = nullptr;
+  if (ncoefs < 1 || !coefs || !offsets || !size || !neighbors)
+    return set_error(GFD_EINVAL, "operator needs at least one coefficient and all arrays");
+  gfd_operator* op = new (std::nothrow) gfd_operator();
+  if (!op) return set_error(GFD_ENOMEM, "host allocation failed");
+  op->ncoefs = ncoefs;
+  op->coefs.assign(coefs, coefs + ncoefs);
+  op->off.resize(3 * ncoefs);
+  op->real = real ? 1 : 0;
+  op->cfd = cfd ? 1 : 0;
+  int mp = 0;
+  for (int c = 0; c < ncoefs; c++)
+    for (int a = 0; a < 3; a++) {
+      int64_t o = offsets[3 * c + a];
+      if (o < -kMaxR * 4 || o > kMaxR * 4) {
+        delete op;
+        return set_error(GFD_EINVAL, "stencil offset out of range");
+      }
+      op->off[3 * c + a] = (int)o;
+      mp = std::max(mp, (int)std::llabs(o));
+    }
+  op->mp = mp;
+  if (range < mp) {
+    delete op;
+    return set_error(GFD_EINVAL, "range is smaller than the largest offset");
+  }
+  for (int a = 0; a < 3; a++) {
+    if (size[a] < 1 || size[a] > (1 << 20)) {
+      delete op;
+      return set_error(GFD_EINVAL, "grid size out of range");
+    }
+    op->n[a] = (int)size[a];
+    int64_t lo = neighbors[2 * a], hi = neighbors[2 * a + 1];
+    if (!((lo == 0 && hi == 0) || (lo == -1 && hi == -1))) {
+      delete op;
+      return set_error(GFD_EUNSUPPORTED,
+                       "neighbors must be 0 (periodic, this domain) or -1 (zero boundary); "
+                       "domain decomposition is not provided");
+    }
+    op->per[a] = (lo == 0) ? 1 : 0;
+    if (op->per[a] && op->n[a] < mp) {
+      delete op;
+      return set_error(GFD_EINVAL, "periodic axis has fewer points than the stencil range");
+    }
+  }
+  if ((double)op->n[0] * op->n[1] * op->n[2] >= 2147483647.0 / 16) {
+    delete op;
+    return set_error(GFD_EINVAL, "grid too large for one band");
+  }
+  // Zero-offset weight (the reference scans for offset 0, c/operators.c:414-417).
+  for (int c = 0; c < ncoefs; c++)
+    if (op->off[3 * c] == 0 && op->off[3 * c + 1] == 0 && op->off[3 * c + 2] == 0)
+      op->diag = coefs[c];
+  // Axis-aligned decomposition.
+  bool star = mp <= kMaxR;
+  for (int c = 0; c < ncoefs && star; c++) {
+    int nz = (op->off[3 * c] != 0) + (op->off[3 * c + 1] != 0) + (op->off[3 * c + 2] != 0);
+    if (nz > 1) star = false;
+  }
+  if (star) {
+    op->c0 = 0.0;
+    for (int c = 0; c < ncoefs; c++) {
+      const int* o = &op->off[3 * c];
+      if (o[0]) op->cx[kMaxR + o[0]] += coefs[c];
+      else if (o[1]) op->cy[kMaxR + o[1]] += coefs[c];
+      else if (o[2]) op->cz[kMaxR + o[2]] += coefs[c];
+      else op->c0 += coefs[c];
+    }
+    op->R = std::max(mp, 1);
+  }
+  op->star = star;
+  *out = op;
+  return GFD_OK;
+}
+
+extern "C" int gfd_operator_destroy(gfd_operator* op) {
+  if (!op) return GFD_OK;
+  if (op->scratch) cudaFree(op->scratch);
+  delete op;
+  return GFD_OK;
+}
+
+extern "C" int gfd_operator_apply(gfd_operator* op, int dtype, const void* in, void* out,
+                                  int64_t nin, const double* phase_cd, void* stream) {
+  if (!op) return set_error(GFD_EINVAL, "null operator");
+  int st = check_dtype(op, dtype);
+  if (st) return st;
+  if (nin < 0) return set_error(GFD_EINVAL, "negative band count");
+  if (nin == 0) return GFD_OK;
+  if (!in || !out) return set_error(GFD_EINVAL, "null array pointer");
+  if (in == out) return set_error(GFD_EINVAL, "input and output must not overlap");
+  return op_launch(op, dtype, OP_APPLY, in, out, nullptr, nin, phase_cd, 0.0, nullptr,
+                   static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method, void* func,
+                                  const void* source, int nrelax, double w, void* stream) {
+  if (!op) return set_error(GFD_EINVAL, "null operator");
+  if (dtype != GFD_FLOAT64 && dtype != GFD_FLOAT32)
+    return set_error(GFD_EINVAL, "relaxation works on real arrays only");
+  if (!op->real) return set_error(GFD_EINVAL, "operator was built for complex arrays");
+  if (!func || !source) return set_error(GFD_EINVAL, "null array pointer");
+  if (nrelax < 0) return set_error(GFD_EINVAL, "negative sweep count");
+  if (nrelax == 0) return GFD_OK;
+  if (op->off[0] != 0 || op->off[1] != 0 || op->off[2] != 0)
+    return set_error(GFD_EINVAL, "relaxation needs the diagonal (zero offset) as coefs[0]");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = (size_t)op->n[0] * op->n[1] * op->n[2] * dtype_size(dtype);
+  int st = ensure_scratch(op, bytes);
+  if (st) return st;
+  if (relax_method == GFD_RELAX_GS) return op_gs_sweeps(op, dtype, func, source, nrelax, op->scratch, s);
+  // Weighted Jacobi: ping-pong between func and the scratch grid.
+  void* cur = func;
+  void* nxt = op->scratch;
+  for (int k = 0; k < nrelax; k++) {
+    st = op_launch(op, dtype, OP_JACOBI, cur, nxt, source, 1, nullptr, w, nullptr, s);
+    if (st) return st;
+    std::swap(cur, nxt);
+  }
+  if (cur != func)
+    return check_cuda(cudaMemcpyAsync(func, cur, bytes, cudaMemcpyDeviceToDevice, s),
+                      "cudaMemcpyAsync(relax result)");
+  return GFD_OK;
+}
+
+extern "C" int gfd_operator_get_diagonal_element(const gfd_operator* op, double* d) {
+  if (!op || !d) return set_error(GFD_EINVAL, "null argument");
+  *d = op->diag;
+  return GFD_OK;
+}

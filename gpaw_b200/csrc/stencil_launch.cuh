@@ -1,0 +1,254 @@
+// stencil_launch.cuh -- host-side tile selection and template dispatch for the
+// stencil kernels.  Included by one translation unit per element type so the
+// instantiations compile in parallel.
+#pragma once
+
+#include <algorithm>
+
+#include "internal.h"
+#include "stencil.cuh"
+
+namespace gfd {
+
+// Tile shapes (BZ x TY threads, VY rows per thread, D planes of prefetch).
+// Wide tiles for grids whose fastest axis fills a warp, narrow ones for the
+// small coarse multigrid levels.
+enum { TILE_WIDE = 0, TILE_MID = 1, TILE_NARROW = 2 };
+
+inline int pick_tile(const gfd_operator* op) {
+  if (op->R > 2) return TILE_WIDE;
+  if (op->n[2] <= 8) return TILE_NARROW;
+  if (op->n[2] <= 16) return TILE_MID;
+  return TILE_WIDE;
+}
+
+struct TileDims {
+  int BZ, BY, NT;
+};
+inline TileDims tile_dims(int tile) {
+  switch (tile) {
+    case TILE_NARROW: return {8, 8, 64};
+    case TILE_MID: return {16, 16, 128};
+    default: return {32, 16, 256};
+  }
+}
+
+struct LaunchGeom {
+  dim3 grid;
+  int nxc, x_chunk;
+  int64_t bands_per_launch;
+};
+
+inline LaunchGeom star_geom(const gfd_operator* op, int tile, int64_t nin, int R) {
+  TileDims td = tile_dims(tile);
+  LaunchGeom g;
+  int gx = (op->n[2] + td.BZ - 1) / td.BZ;
+  int gy = (op->n[1] + td.BY - 1) / td.BY;
+  int64_t tiles = (int64_t)gx * gy * std::max<int64_t>(nin, 1);
+  int64_t target = 4LL * num_sms();
+  int maxc = std::max(1, op->n[0] / std::max(4, 2 * R));
+  int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
+  g.x_chunk = (op->n[0] + nxc - 1) / nxc;
+  g.nxc = (op->n[0] + g.x_chunk - 1) / g.x_chunk;
+  g.bands_per_launch = std::max<int64_t>(1, 65535 / g.nxc);
+  g.grid = dim3(gx, gy, 1);
+  return g;
+}
+
+template <class S>
+void fill_phases(Phases<S>& P, const double* ph) {
+  for (int c = 0; c < 3; c++)
+    for (int d = 0; d < 2; d++) {
+      P.ph[c][d].re = ph ? S(ph[4 * c + 2 * d]) : S(1);
+      P.ph[c][d].im = ph ? S(ph[4 * c + 2 * d + 1]) : S(0);
+    }
+}
+
+template <class V, int R, int BZ, int TY, int VY, int MODE>
+int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
+            const StarParams<typename vt<V>::S>& base, const LaunchGeom& g, double* partials,
+            cudaStream_t s) {
+  constexpr int D = 2;
+  StarParams<typename vt<V>::S> p = base;
+  const long long band = (long long)op->n[0] * op->n[1] * op->n[2];
+  for (int64_t b0 = 0; b0 < nin; b0 += g.bands_per_launch) {
+    int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
+    dim3 grid(g.grid.x, g.grid.y, (unsigned)(nb * g.nxc));
+    p.partials = partials ? partials + b0 * g.nxc * g.grid.x * g.grid.y : nullptr;
+    star_kernel<V, R, BZ, TY, VY, D, MODE><<<grid, BZ * TY, 0, s>>>(
+        in + b0 * band, out + b0 * band, rho ? rho + b0 * band : nullptr, p);
+  }
+  return check_launch("star_kernel");
+}
+
+template <class V, int MODE>
+int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V* rho, int64_t nin,
+                  const StarParams<typename vt<V>::S>& p, const LaunchGeom& g, double* partials,
+                  cudaStream_t s) {
+#define GFD_STAR_SMALL(RR)                                                                   \
+  case RR:                                                                                   \
+    if (tile == TILE_NARROW)                                                                 \
+      return star_go<V, RR, 8, 8, 1, MODE>(op, in, out, rho, nin, p, g, partials, s);        \
+    if (tile == TILE_MID)                                                                    \
+      return star_go<V, RR, 16, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);       \
+    return star_go<V, RR, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+#define GFD_STAR_WIDE(RR) \
+  case RR:                \
+    return star_go<V, RR, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+  switch (op->R) {
+    GFD_STAR_SMALL(1)
+    GFD_STAR_SMALL(2)
+    GFD_STAR_WIDE(3)
+    GFD_STAR_WIDE(4)
+    GFD_STAR_WIDE(5)
+    GFD_STAR_WIDE(6)
+  }
+#undef GFD_STAR_SMALL
+#undef GFD_STAR_WIDE
+  return set_error(GFD_EUNSUPPORTED, "star stencil radius out of range");
+}
+
+template <class V>
+int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* out, const void* rho,
+                      int64_t nin, const double* phase_cd, double w, double* partials,
+                      cudaStream_t s) {
+  using S = typename vt<V>::S;
+  StarParams<S> p{};
+  p.n0 = op->n[0]; p.n1 = op->n[1]; p.n2 = op->n[2];
+  p.per0 = op->per[0]; p.per1 = op->per[1]; p.per2 = op->per[2];
+  p.band = (long long)op->n[0] * op->n[1] * op->n[2];
+  p.c0 = S(op->c0);
+  for (int i = 0; i < 2 * kMaxR + 1; i++) {
+    p.cx[i] = S(op->cx[i]);
+    p.cy[i] = S(op->cy[i]);
+    p.cz[i] = S(op->cz[i]);
+  }
+  p.w = S(w);
+  fill_phases(p.P, phase_cd);
+  const int tile = pick_tile(op);
+  LaunchGeom g = star_geom(op, tile, nin, op->R);
+  p.nxc = g.nxc;
+  p.x_chunk = g.x_chunk;
+  const V* vin = static_cast<const V*>(in);
+  V* vout = static_cast<V*>(out);
+  const V* vrho = static_cast<const V*>(rho);
+  if constexpr (vt<V>::NC == 1) {
+    if (mode == OP_JACOBI)
+      return star_dispatch<V, MODE_JACOBI>(op, tile, vin, vout, vrho, nin, p, g, nullptr, s);
+    if (mode == OP_RESIDUAL)
+      return star_dispatch<V, MODE_RESIDUAL>(op, tile, vin, vout, vrho, nin, p, g, partials, s);
+  } else {
+    if (mode != OP_APPLY) return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
+  }
+  return star_dispatch<V, MODE_APPLY>(op, tile, vin, vout, nullptr, nin, p, g, nullptr, s);
+}
+
+template <class V, int MODE>
+int general_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
+               GenParams<typename vt<V>::S>& p, double* partials, cudaStream_t s) {
+  constexpr int BZ = 32, TY = 4, VY = 2, BY = TY * VY;
+  const int mp = std::max(op->mp, 0);
+  const int gx = (op->n[2] + BZ - 1) / BZ, gy = (op->n[1] + BY - 1) / BY;
+  gfd_operator tmp = *op;
+  tmp.scratch = nullptr;  // geometry only
+  LaunchGeom g = star_geom(op, TILE_WIDE, nin, std::max(mp, 1));
+  g.grid = dim3(gx, gy, 1);
+  p.nxc = g.nxc;
+  p.x_chunk = g.x_chunk;
+  size_t smem = (size_t)(2 * mp + 1) * (BY + 2 * mp) * (BZ + 2 * mp) * sizeof(V);
+  if (smem > 227 * 1024) return set_error(GFD_EUNSUPPORTED, "stencil range too large");
+  cudaError_t e = cudaFuncSetAttribute(general_kernel<V, BZ, TY, VY, MODE>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(general_kernel)");
+  const long long band = (long long)op->n[0] * op->n[1] * op->n[2];
+  for (int64_t b0 = 0; b0 < nin; b0 += g.bands_per_launch) {
+    int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
+    dim3 grid(gx, gy, (unsigned)(nb * g.nxc));
+    p.partials = partials ? partials + b0 * g.nxc * gx * gy : nullptr;
+    general_kernel<V, BZ, TY, VY, MODE><<<grid, BZ * TY, smem, s>>>(
+        in + b0 * band, out + b0 * band, rho ? rho + b0 * band : nullptr, p, mp);
+  }
+  return check_launch("general_kernel");
+}
+
+template <class V>
+int launch_general_typed(const gfd_operator* op, int mode, const void* in, void* out,
+                         const void* rho, int64_t nin, const double* phase_cd, double w,
+                         double* partials, cudaStream_t s) {
+  using S = typename vt<V>::S;
+  if (op->ncoefs > kMaxCoefs) return set_error(GFD_EUNSUPPORTED, "too many stencil coefficients");
+  GenParams<S> p{};
+  p.n0 = op->n[0]; p.n1 = op->n[1]; p.n2 = op->n[2];
+  p.per0 = op->per[0]; p.per1 = op->per[1]; p.per2 = op->per[2];
+  p.band = (long long)op->n[0] * op->n[1] * op->n[2];
+  p.ncoefs = op->ncoefs;
+  for (int c = 0; c < op->ncoefs; c++) {
+    p.coefs[c] = S(op->coefs[c]);
+    for (int a = 0; a < 3; a++) p.off[c][a] = (signed char)op->off[3 * c + a];
+  }
+  p.w = S(w);
+  fill_phases(p.P, phase_cd);
+  const V* vin = static_cast<const V*>(in);
+  V* vout = static_cast<V*>(out);
+  const V* vrho = static_cast<const V*>(rho);
+  if constexpr (vt<V>::NC == 1) {
+    if (mode == OP_JACOBI) return general_go<V, MODE_JACOBI>(op, vin, vout, vrho, nin, p, nullptr, s);
+    if (mode == OP_RESIDUAL)
+      return general_go<V, MODE_RESIDUAL>(op, vin, vout, vrho, nin, p, partials, s);
+  } else {
+    if (mode != OP_APPLY) return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
+  }
+  return general_go<V, MODE_APPLY>(op, vin, vout, nullptr, nin, p, nullptr, s);
+}
+
+inline int64_t partials_count(const gfd_operator* op, int64_t nin) {
+  if (op->star) {
+    int tile = pick_tile(op);
+    TileDims td = tile_dims(tile);
+    LaunchGeom g = star_geom(op, tile, nin, op->R);
+    int gx = (op->n[2] + td.BZ - 1) / td.BZ, gy = (op->n[1] + td.BY - 1) / td.BY;
+    return (int64_t)gx * gy * g.nxc * nin;
+  }
+  const int BZ = 32, BY = 8;
+  LaunchGeom g = star_geom(op, TILE_WIDE, nin, std::max(op->mp, 1));
+  int gx = (op->n[2] + BZ - 1) / BZ, gy = (op->n[1] + BY - 1) / BY;
+  return (int64_t)gx * gy * g.nxc * nin;
+}
+
+template <class V>
+int gs_typed(const gfd_operator* op, V* phi, const V* rho, int nsweeps, V* frozen, int ncolor,
+             cudaStream_t s) {
+  using S = typename vt<V>::S;
+  GenParams<S> p{};
+  p.n0 = op->n[0]; p.n1 = op->n[1]; p.n2 = op->n[2];
+  p.per0 = op->per[0]; p.per1 = op->per[1]; p.per2 = op->per[2];
+  p.band = (long long)op->n[0] * op->n[1] * op->n[2];
+  p.ncoefs = op->ncoefs;
+  for (int c = 0; c < op->ncoefs; c++) {
+    p.coefs[c] = S(op->coefs[c]);
+    for (int a = 0; a < 3; a++) p.off[c][a] = (signed char)op->off[3 * c + a];
+  }
+  const long long n = p.band;
+  const bool any_per = op->per[0] || op->per[1] || op->per[2];
+  int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  for (int sw = 0; sw < nsweeps; sw++) {
+    if (any_per) {
+      cudaError_t e = cudaMemcpyAsync(frozen, phi, n * sizeof(V), cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return check_cuda(e, "cudaMemcpyAsync(frozen)");
+    }
+    for (int c = 0; c < ncolor; c++)
+      color_gs_kernel<V><<<blocks, 256, 0, s>>>(phi, rho, any_per ? frozen : phi, p, ncolor, c);
+  }
+  return check_launch("color_gs_kernel");
+}
+
+}  // namespace gfd
+
+// One of these per element type, defined in stencil_<type>.cu.
+#define GFD_DECLARE_STENCIL_ENTRY(NAME)                                                        \
+  namespace gfd {                                                                             \
+  int star_##NAME(const gfd_operator*, int, const void*, void*, const void*, int64_t,          \
+                  const double*, double, double*, cudaStream_t);                              \
+  int general_##NAME(const gfd_operator*, int, const void*, void*, const void*, int64_t,       \
+                     const double*, double, double*, cudaStream_t);                           \
+  }

@@ -1,0 +1,319 @@
+// transfer.cuh -- multigrid restriction and interpolation for sm_100a.
+//
+// The reference (c/bmgs/restrict.c, c/bmgs/interpolate.c, driven by
+// c/transformers.c:54-123) fills a halo-padded copy of each band and then
+// runs three transposing 1-D passes (axis 2, axis 1, axis 0) through scratch
+// buffers: about four reads and four writes of the array.  Here one kernel
+// does all three passes:
+//   * a CTA owns a tile of output points in (axis 1, axis 2) and marches
+//     along axis 0;
+//   * each input plane (with its halo, mapped in-kernel: zero, periodic, or
+//     periodic times the Bloch phase) is staged in shared memory, the axis-2
+//     pass and then the axis-1 pass run there (the reference's pass order,
+//     so the arithmetic matches term by term);
+//   * the axis-0 pass reads a per-thread register queue of the last planes'
+//     2-D results.
+// HBM traffic is one read of the input and one write of the output.
+//
+// Weights: Lagrange weights for K = 2*nn taps (c/bmgs/restrict.c:37-57,
+// c/bmgs/interpolate.c:46-59).
+#pragma once
+
+#include "common.cuh"
+
+namespace gfd {
+
+template <int NN, class S> __device__ __forceinline__ S lagw(int m);
+template <int NN, class S>
+__device__ __forceinline__ S lagw(int m) {
+  if (NN == 1) return S(0.5);
+  if (NN == 2) return m == 0 ? S(0.5625) : S(-0.0625);
+  if (NN == 3) return m == 0 ? S(0.58593750) : (m == 1 ? S(-0.09765625) : S(0.01171875));
+  return m == 0 ? S(0.59814453125)
+                : (m == 1 ? S(-0.11962890625) : (m == 2 ? S(0.02392578125) : S(-0.00244140625)));
+}
+
+// Restriction tap around a[0] with stride st (in elements of V):
+// 0.5 * (a0 + w1 (a[+1] + a[-1]) + w2 (a[+3] + a[-3]) + ...)
+template <int NN, class V, class Get>
+__device__ __forceinline__ V rst_tap(Get get) {
+  using S = typename vt<V>::S;
+  V x = get(0);
+#pragma unroll
+  for (int k = 0; k < NN; k++) x = vadd(x, vmul(lagw<NN, S>(k), vadd(get(2 * k + 1), get(-(2 * k + 1)))));
+  return vmul(S(0.5), x);
+}
+
+// Interpolated value between a[0] and a[1]:
+// w0 (a[0] + a[1]) + w1 (a[-1] + a[2]) + ...
+template <int NN, class V, class Get>
+__device__ __forceinline__ V ip_tap(Get get) {
+  using S = typename vt<V>::S;
+  V x = vmul(lagw<NN, S>(0), vadd(get(0), get(1)));
+#pragma unroll
+  for (int m = 1; m < NN; m++) x = vadd(x, vmul(lagw<NN, S>(m), vadd(get(-m), get(1 + m))));
+  return x;
+}
+
+template <class S>
+struct TrParams {
+  int ni0, ni1, ni2;   // input points per axis
+  int no0, no1, no2;   // output points per axis
+  int lo0, lo1, lo2;   // low-side padding of the input (pad[c][0])
+  int sk0, sk1, sk2;   // interpolation: skip[c][0]
+  int per0, per1, per2;
+  int x_chunk, nxc;    // output planes per CTA along axis 0, chunk count
+  long long band_in, band_out;
+  Phases<S> P;
+};
+
+// Pack an in-plane source offset and its wrap sides; -1 = zero point.
+__device__ __forceinline__ int pack_src(int ys, int zs, int n2, int ysd, int zsd) {
+  if (ys < 0 || zs < 0) return -1;
+  return ((ys * n2 + zs) << 4) | ((ysd + 1) | ((zsd + 1) << 2));
+}
+
+template <class V, class S>
+__device__ __forceinline__ V apply_phases(V v, int code, int xside, const Phases<S>& P) {
+  if constexpr (vt<V>::NC == 2) {
+    if (xside >= 0) v = phase_mul(phase_of(P, 0, xside), v);
+    int ys = (code & 3) - 1, zs = ((code >> 2) & 3) - 1;
+    if (ys >= 0) v = phase_mul(phase_of(P, 1, ys), v);
+    if (zs >= 0) v = phase_mul(phase_of(P, 2, zs), v);
+  }
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Restriction: coarse index i on an axis takes the fine padded point
+// (K-1) + 2i (c/bmgs/restrict.c:65-69), i.e. fine array index
+// 2i + (2nn-1) - lo.
+// ---------------------------------------------------------------------------
+template <class V, int NN, int BZC, int TYC, int VYC>
+__global__ void __launch_bounds__(BZC * TYC)
+restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
+                const TrParams<typename vt<V>::S> p) {
+  using S = typename vt<V>::S;
+  constexpr int NT = BZC * TYC, BYC = TYC * VYC;
+  constexpr int W = 2 * NN - 1;           // wing of one restriction tap
+  constexpr int RY = 2 * BYC - 1 + 2 * W;
+  constexpr int RZ = 2 * BZC - 1 + 2 * W;
+  constexpr int CELLS = RY * RZ;
+  constexpr int CC = (CELLS + NT - 1) / NT;
+  constexpr int QL = 2 * W + 1;           // fine planes feeding one coarse plane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZ]
+  V* T = F + 2 * CELLS;                           // [2][RY][BZC]
+
+  const int t = threadIdx.x, tz = t % BZC, ty = t / BZC;
+  const int Z0 = blockIdx.x * BZC, Y0 = blockIdx.y * BYC;
+  const int bnd = blockIdx.z / p.nxc, xc = blockIdx.z % p.nxc;
+  const int X0 = xc * p.x_chunk, X1 = min(p.no0, X0 + p.x_chunk);
+  const long long plane_in = (long long)p.ni1 * p.ni2;
+  const long long plane_out = (long long)p.no1 * p.no2;
+  const V* inb = in + bnd * p.band_in;
+  V* outb = out + bnd * p.band_out;
+  const int fy0 = 2 * Y0 - p.lo1, fz0 = 2 * Z0 - p.lo2;
+
+  int src[CC];
+#pragma unroll
+  for (int i = 0; i < CC; i++) {
+    int c = t + i * NT;
+    src[i] = -1;
+    if (c < CELLS) {
+      int sy = c / RZ, sz = c % RZ;
+      int ysd, zsd;
+      int ys = wrap_axis(fy0 + sy, p.ni1, p.per1, ysd);
+      int zs = wrap_axis(fz0 + sz, p.ni2, p.per2, zsd);
+      src[i] = pack_src(ys, zs, p.ni2, ysd, zsd);
+    }
+  }
+
+  const int fbeg = 2 * X0 + W - p.lo0 - W;
+  const int fend = 2 * (X1 - 1) + W - p.lo0 + W + 1;
+
+  V rv[CC];
+  auto load = [&](int f) {
+    int xside;
+    int xs = (f < fend) ? wrap_axis(f, p.ni0, p.per0, xside) : -1;
+#pragma unroll
+    for (int i = 0; i < CC; i++) {
+      V v = vzero<V>();
+      if (xs >= 0 && src[i] >= 0) {
+        v = ldro(inb + xs * plane_in + (src[i] >> 4));
+        v = apply_phases<V, S>(v, src[i] & 15, xside, p.P);
+      }
+      rv[i] = v;
+    }
+  };
+
+  V q[VYC][QL];
+#pragma unroll
+  for (int j = 0; j < VYC; j++)
+#pragma unroll
+    for (int k = 0; k < QL; k++) q[j][k] = vzero<V>();
+
+  load(fbeg);
+  for (int f = fbeg; f < fend; ++f) {
+    V* Fb = F + (f & 1) * CELLS;
+    V* Tb = T + (f & 1) * RY * BZC;
+#pragma unroll
+    for (int i = 0; i < CC; i++)
+      if (t + i * NT < CELLS) Fb[t + i * NT] = rv[i];
+    load(f + 1);
+    __syncthreads();
+    // axis-2 pass: Tb[sy][cz] for every staged row
+    for (int c = t; c < RY * BZC; c += NT) {
+      const int sy = c / BZC, cz = c % BZC;
+      const V* row = Fb + sy * RZ + 2 * cz + W;
+      Tb[c] = rst_tap<NN, V>([&](int o) { return row[o]; });
+    }
+    __syncthreads();
+    // axis-1 pass for this thread's coarse points, pushed into the queue
+#pragma unroll
+    for (int j = 0; j < VYC; j++) {
+      const V* col = Tb + (2 * (ty + j * TYC) + W) * BZC + tz;
+      V v = rst_tap<NN, V>([&](int o) { return col[o * BZC]; });
+#pragma unroll
+      for (int k = 0; k + 1 < QL; k++) q[j][k] = q[j][k + 1];
+      q[j][QL - 1] = v;
+    }
+    // axis-0 pass: the queue centre is fine plane f - W
+    const int fc = f - W;
+    const int rel = fc - W + p.lo0;
+    if (f - fbeg >= QL - 1 && (rel & 1) == 0) {
+      const int X = rel >> 1;
+      if (X >= X0 && X < X1) {
+#pragma unroll
+        for (int j = 0; j < VYC; j++) {
+          const int y = Y0 + ty + j * TYC, z = Z0 + tz;
+          if (y < p.no1 && z < p.no2) {
+            V v = rst_tap<NN, V>([&](int o) { return q[j][W + o]; });
+            stcs(outb + X * plane_out + (long long)y * p.no2 + z, v);
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Interpolation: fine index f on an axis has g = f + skip[c][0]; g = 2i is a
+// copy of coarse padded point (nn-1) + i, g = 2i + 1 the K-tap value between
+// (nn-1) + i and (nn-1) + i + 1 (c/bmgs/interpolate.c:19-66).  Coarse array
+// index of step i: c(i) = i + nn - 1 - lo.
+// ---------------------------------------------------------------------------
+template <class V, int NN, int BZF, int TYF, int VYF>
+__global__ void __launch_bounds__(BZF * TYF)
+interp_kernel(const V* __restrict__ in, V* __restrict__ out,
+              const TrParams<typename vt<V>::S> p) {
+  using S = typename vt<V>::S;
+  constexpr int NT = BZF * TYF, BYF = TYF * VYF;
+  constexpr int CY = BYF / 2 + 2 * NN, CZ = BZF / 2 + 2 * NN;
+  constexpr int CELLS = CY * CZ;
+  constexpr int CC = (CELLS + NT - 1) / NT;
+  constexpr int QL = 2 * NN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* C = reinterpret_cast<V*>(smem_raw);  // [2][CY][CZ]
+  V* T = C + 2 * CELLS;                   // [2][CY][BZF]
+
+  const int t = threadIdx.x, tz = t % BZF, ty = t / BZF;
+  const int Z0 = blockIdx.x * BZF, Y0 = blockIdx.y * BYF;
+  const int bnd = blockIdx.z / p.nxc, xc = blockIdx.z % p.nxc;
+  const int X0 = xc * p.x_chunk, X1 = min(p.no0, X0 + p.x_chunk);
+  const long long plane_in = (long long)p.ni1 * p.ni2;
+  const long long plane_out = (long long)p.no1 * p.no2;
+  const V* inb = in + bnd * p.band_in;
+  V* outb = out + bnd * p.band_out;
+  const int iy0 = (Y0 + p.sk1) >> 1, iz0 = (Z0 + p.sk2) >> 1;
+  const int cy0 = iy0 - p.lo1, cz0 = iz0 - p.lo2;  // coarse origin of the tile
+
+  int src[CC];
+#pragma unroll
+  for (int i = 0; i < CC; i++) {
+    int c = t + i * NT;
+    src[i] = -1;
+    if (c < CELLS) {
+      int sy = c / CZ, sz = c % CZ;
+      int ysd, zsd;
+      int ys = wrap_axis(cy0 + sy, p.ni1, p.per1, ysd);
+      int zs = wrap_axis(cz0 + sz, p.ni2, p.per2, zsd);
+      src[i] = pack_src(ys, zs, p.ni2, ysd, zsd);
+    }
+  }
+
+  const int ia = (X0 + p.sk0) >> 1, ib = (X1 - 1 + p.sk0) >> 1;
+  const int cbeg = ia - p.lo0;                    // c(ia) - (nn-1)
+  const int cend = ib + NN - 1 - p.lo0 + NN + 1;  // one past c(ib) + nn
+
+  V rv[CC];
+  auto load = [&](int c) {
+    int xside;
+    int xs = (c < cend) ? wrap_axis(c, p.ni0, p.per0, xside) : -1;
+#pragma unroll
+    for (int i = 0; i < CC; i++) {
+      V v = vzero<V>();
+      if (xs >= 0 && src[i] >= 0) {
+        v = ldro(inb + xs * plane_in + (src[i] >> 4));
+        v = apply_phases<V, S>(v, src[i] & 15, xside, p.P);
+      }
+      rv[i] = v;
+    }
+  };
+
+  V q[VYF][QL];
+#pragma unroll
+  for (int j = 0; j < VYF; j++)
+#pragma unroll
+    for (int k = 0; k < QL; k++) q[j][k] = vzero<V>();
+
+  load(cbeg);
+  for (int c = cbeg; c < cend; ++c) {
+    V* Cb = C + (c & 1) * CELLS;
+    V* Tb = T + (c & 1) * CY * BZF;
+#pragma unroll
+    for (int i = 0; i < CC; i++)
+      if (t + i * NT < CELLS) Cb[t + i * NT] = rv[i];
+    load(c + 1);
+    __syncthreads();
+    // axis-2 pass: every staged coarse row to this tile's fine columns
+    for (int e = t; e < CY * BZF; e += NT) {
+      const int sy = e / BZF, fz = e % BZF;
+      const int g = Z0 + fz + p.sk2;
+      const int cl = (g >> 1) - iz0 + NN - 1;
+      const V* row = Cb + sy * CZ + cl;
+      Tb[e] = (g & 1) ? ip_tap<NN, V>([&](int o) { return row[o]; }) : row[0];
+    }
+    __syncthreads();
+    // axis-1 pass for this thread's fine points
+#pragma unroll
+    for (int j = 0; j < VYF; j++) {
+      const int g = Y0 + ty + j * TYF + p.sk1;
+      const int cl = (g >> 1) - iy0 + NN - 1;
+      const V* col = Tb + cl * BZF + tz;
+      V v = (g & 1) ? ip_tap<NN, V>([&](int o) { return col[o * BZF]; }) : col[0];
+#pragma unroll
+      for (int k = 0; k + 1 < QL; k++) q[j][k] = q[j][k + 1];
+      q[j][QL - 1] = v;
+    }
+    // axis-0 pass: step i with c(i) + nn == c emits fine g = 2i and 2i + 1
+    const int i = c - 2 * NN + 1 + p.lo0;
+    if (c - cbeg >= QL - 1 && i >= ia && i <= ib) {
+#pragma unroll
+      for (int par = 0; par < 2; par++) {
+        const int X = 2 * i + par - p.sk0;
+        if (X < X0 || X >= X1) continue;
+#pragma unroll
+        for (int j = 0; j < VYF; j++) {
+          const int y = Y0 + ty + j * TYF, z = Z0 + tz;
+          if (y < p.no1 && z < p.no2) {
+            V v = par ? ip_tap<NN, V>([&](int o) { return q[j][NN - 1 + o]; }) : q[j][NN - 1];
+            stcs(outb + X * plane_out + (long long)y * p.no2 + z, v);
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace gfd

@@ -1,0 +1,87 @@
+// util.cuh -- small streaming kernels: update, conversion, deterministic
+// reductions.  All grid-stride loops use 128-bit accesses where the type
+// allows; reductions run over a fixed grid so their summation order, and
+// hence their result, does not depend on timing.
+#pragma once
+
+#include "common.cuh"
+
+namespace gfd {
+
+constexpr int kRedBlocks = 1184;  // 8 per SM on 148 SMs
+constexpr int kRedThreads = 256;
+
+// y[i] = a * y[i] + b * x[i]   (mixed types allowed: X may be float)
+template <class Y, class X>
+__global__ void __launch_bounds__(256) axpby_kernel(Y* __restrict__ y, const X* __restrict__ x,
+                                                    double a, double b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = Y(a * double(y[i]) + b * double(x[i]));
+}
+
+// y[i] = x[i] - c  (background removal; y may alias x)
+template <class T>
+__global__ void __launch_bounds__(256) sub_const_kernel(T* y, const T* x, double c, long long n) {
+  const T cc = T(c);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = x[i] - cc;
+}
+
+// y[i] = T(x[i])
+template <class Y, class X>
+__global__ void __launch_bounds__(256) convert_kernel(Y* __restrict__ y, const X* __restrict__ x,
+                                                      long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = Y(x[i]);
+}
+
+// Per-block partial sums of a[i] (SQUARE: a[i]^2), in a fixed order.
+template <class T, bool SQUARE>
+__global__ void __launch_bounds__(kRedThreads) partial_sum_kernel(const T* __restrict__ a,
+                                                                  long long n,
+                                                                  double* __restrict__ partials) {
+  __shared__ double red[kRedThreads / 32];
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kRedThreads) {
+    double v = double(a[i]);
+    s += SQUARE ? v * v : v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int w = 0; w < kRedThreads / 32; w++) b += red[w];
+    partials[blockIdx.x] = b;
+  }
+}
+
+// out[0] = scale * sum(partials[0..n)), one block, fixed tree order.
+static __global__ void __launch_bounds__(kRedThreads) final_sum_kernel(const double* __restrict__ partials,
+                                                                int n, double scale,
+                                                                double* __restrict__ out) {
+  __shared__ double red[kRedThreads];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += kRedThreads) s += partials[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0] * scale;
+}
+
+// Launch helpers (host).
+inline int grid_for(long long n, int threads = 256, int max_blocks = 148 * 16) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return int(b);
+}
+
+}  // namespace gfd

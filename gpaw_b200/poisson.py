@@ -1,0 +1,151 @@
+"""Multigrid Poisson solver on the GPU (drop-in for gpaw.poisson.PoissonSolver).
+
+PoissonSolver(nn=3, relax='J', eps=2e-10) with set_grid_descriptor(gd),
+initialize() and solve(phi, rho, charge=None, eps=None, maxcharge=1e-6,
+zero_initial_phi=False) -> number of V-cycles, as gpaw/poisson.py:21-218.
+The level hierarchy is the reference's (gpaw/poisson.py:45-89, 111-113):
+
+  level 0      Laplace(gd, -1/(4 pi), nn), 2 pre- / 1 post-smoothing sweeps,
+               Jacobi weight 2/3
+  levels 1..L  Laplace(gd_l, -1/(4 pi), 1), 4 / 4 sweeps, weight 1, at most
+               four coarsenings; the coarsest level smooths 8 / 8 times
+  transfers    Transformer(nn=1) restriction and interpolation
+
+relax='J' is weighted Jacobi as in the reference; relax='GS' is multicolour
+Gauss-Seidel (the reference's lexicographic sweep is sequential).  The whole
+V-cycle, the residual norm and the convergence test run in libgpawfd on the
+device; phi and rho are float64 CUDA tensors.
+
+precision='mixed' keeps the float64 residual, update and norm and runs the
+V-cycle in float32 (defect correction); precision='fp64' is the plain form.
+"""
+from math import pi
+
+import numpy as np
+
+from . import _lib
+from .errors import PoissonConvergenceError  # noqa: F401  (re-exported)
+from .fd_operators import Laplace
+from .tensors import require_device, stream_of
+from .transformers import Transformer
+
+
+class PoissonSolver:
+    def __init__(self, nn=3, relax='J', eps=2e-10, precision='fp64'):
+        self.relax = relax
+        self.nn = nn
+        self.eps = eps
+        self.maxiter = 1000
+        self.charged_periodic_correction = None
+        if relax == 'GS':
+            self.relax_method = _lib.GFD_RELAX_GS
+        elif relax == 'J':
+            self.relax_method = _lib.GFD_RELAX_JACOBI
+        else:
+            raise NotImplementedError('Relaxation method %s' % relax)
+        if precision not in ('fp64', 'mixed'):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        self.solver = None
+
+    def get_method(self):
+        return ['Gauss-Seidel', 'Jacobi'][self.relax_method - 1]
+
+    def get_stencil(self):
+        return self.nn
+
+    def set_grid_descriptor(self, gd):
+        if self.nn == 'M':
+            raise NotImplementedError('Mehrstellen Poisson (nn="M") is not provided')
+        self.gd = gd
+        self.dv = gd.dv
+        scale = -0.25 / pi
+        self.operators = [Laplace(gd, scale, self.nn, allocate=False)]
+        self.interpolators = []
+        self.restrictors = []
+        self.presmooths = [2]
+        self.postsmooths = [1]
+        self.weights = [2.0 / 3.0]
+        level = 0
+        while level < 4:
+            try:
+                gd2 = gd.coarsen()
+            except ValueError:
+                break
+            self.operators.append(Laplace(gd2, scale, 1, allocate=False))
+            self.interpolators.append(Transformer(gd2, gd, allocate=False))
+            self.restrictors.append(Transformer(gd, gd2, allocate=False))
+            self.presmooths.append(4)
+            self.postsmooths.append(4)
+            self.weights.append(1.0)
+            level += 1
+            gd = gd2
+        self.levels = level
+
+    def initialize(self, load_gauss=False):
+        for obj in self.operators + self.interpolators + self.restrictors:
+            if not obj.allocated:
+                obj.allocate()
+        self.presmooths[self.levels] = 8
+        self.postsmooths[self.levels] = 8
+        self.step = 0.66666666 / self.operators[0].get_diagonal_element()
+        L = self.levels
+        ops = (_lib._vp * (L + 1))(*[o.operator for o in self.operators])
+        rs = (_lib._vp * max(L, 1))(*[t.transformer for t in self.restrictors])
+        ips = (_lib._vp * max(L, 1))(*[t.transformer for t in self.interpolators])
+        pre = (_lib.ctypes.c_int * (L + 1))(*self.presmooths)
+        post = (_lib.ctypes.c_int * (L + 1))(*self.postsmooths)
+        w = (_lib.ctypes.c_double * (L + 1))(*self.weights)
+        handle = _lib._vp()
+        mode = _lib.GFD_POISSON_MIXED if self.precision == 'mixed' else _lib.GFD_POISSON_FP64
+        _lib.check(_lib.lib.gfd_poisson_create(
+            L, ops, rs, ips, pre, post, w, self.relax_method, float(self.gd.dv),
+            int(self.gd.pbc_c.all()), mode, _lib.ctypes.byref(handle)), 'PoissonSolver')
+        self.solver = handle
+
+    def __del__(self):
+        h = getattr(self, 'solver', None)
+        if h:
+            _lib.lib.gfd_poisson_destroy(h)
+            self.solver = None
+
+    def solve(self, phi, rho, charge=None, eps=None, maxcharge=1e-6, zero_initial_phi=False):
+        """Solve nabla^2 phi = -4 pi rho for a charge-neutral rho; phi holds
+        the initial guess and receives the solution.  Returns the number of
+        V-cycles.  Raises PoissonConvergenceError after maxiter V-cycles."""
+        if self.solver is None:
+            self.initialize()
+        require_device(phi, 'phi')
+        require_device(rho, 'rho')
+        import torch
+        if phi.dtype != torch.float64 or rho.dtype != torch.float64:
+            raise ValueError('phi and rho must be float64')
+        shape = tuple(int(x) for x in self.gd.n_c)
+        if tuple(phi.shape) != shape or tuple(rho.shape) != shape:
+            raise ValueError('phi and rho must have the grid shape %s' % (shape,))
+        if eps is None:
+            eps = self.eps
+        if zero_initial_phi:
+            phi.zero_()
+        niter = _lib.ctypes.c_int(0)
+        err = _lib.ctypes.c_double(0.0)
+        status = _lib.lib.gfd_poisson_solve(
+            self.solver, phi.data_ptr(), rho.data_ptr(),
+            _lib.nan() if charge is None else float(charge), float(eps), float(maxcharge),
+            int(self.maxiter), _lib.ctypes.byref(niter), _lib.ctypes.byref(err), stream_of(phi))
+        self.niter = niter.value
+        self.error = err.value
+        _lib.check(status, 'PoissonSolver.solve')
+        return niter.value
+
+    def estimate_memory(self, mem):
+        nbytes = 0
+        g = int(np.prod(self.gd.n_c)) * 8
+        for _ in range(self.levels + 1):
+            nbytes += 4 * g
+            g //= 8
+        mem.subnode('rho, phi (x2), residual [%d levels]' % self.levels, nbytes)
+
+    def __repr__(self):
+        return 'PoissonSolver(relax=\'%s\', nn=%s, eps=%e)' % (self.relax, repr(self.nn),
+                                                              self.eps)

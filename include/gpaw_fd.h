@@ -1,0 +1,187 @@
+/*
+ * gpaw_fd.h -- C ABI of libgpawfd.so, the B200 (sm_100a) implementation of
+ * GPAW's real-space finite-difference path.
+ *
+ * Every entry point takes plain pointers and sizes.  Array arguments named
+ * in/out/func/source/phi/rho are DEVICE pointers to C-contiguous arrays of
+ * shape (nin, n0, n1, n2) (complex values interleaved re, im), exactly the
+ * layout of the numpy arrays the reference passes to its C extension.
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  Work is
+ * enqueued on that stream and the call returns without waiting, except where
+ * a result must reach the host (gfd_poisson_solve, gfd_grid_sum).
+ *
+ * Every call returns a status code; gfd_last_error() gives the message of the
+ * last failing call on the calling thread.  Nothing aborts or traps.
+ *
+ * Reference interfaces replaced (paths relative to the GPAW source tree):
+ *   _gpaw.Operator      c/operators.c:465-498 (constructor), :316-405 (apply),
+ *                       :49-91 (relax), :408-421 (get_diagonal_element)
+ *   _gpaw.Transformer   c/transformers.c:222-265 (constructor), :127-185 (apply)
+ *   PoissonSolver       gpaw/poisson.py:21-276 (set_grid_descriptor,
+ *                       initialize, solve, solve_neutral, iterate2)
+ *   GridDescriptor.integrate  gpaw/grid_descriptor.py:197-215
+ */
+#ifndef GPAW_FD_H
+#define GPAW_FD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GFD_API __attribute__((visibility("default")))
+#else
+#define GFD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define GFD_OK 0
+#define GFD_EINVAL 1      /* bad shape, size, pointer, dtype or argument */
+#define GFD_ENOMEM 2      /* device allocation failed */
+#define GFD_ENOCONV 3     /* Poisson solve reached maxiter (PoissonConvergenceError) */
+#define GFD_ETIMEOUT 4    /* a bounded device-side wait ran out */
+#define GFD_ECUDA 5       /* a CUDA runtime call failed */
+#define GFD_EUNSUPPORTED 6 /* valid in the reference but not provided here */
+
+/* Element types (the `dtype` argument).  The FP32 types are the reduced-
+ * precision variants; the reference computes in float64 / complex128 only. */
+#define GFD_FLOAT64 0
+#define GFD_COMPLEX128 1
+#define GFD_FLOAT32 2
+#define GFD_COMPLEX64 3
+
+/* Relaxation methods, numbered as in gpaw/poisson.py:28-36. */
+#define GFD_RELAX_GS 1      /* Gauss-Seidel; here multicolour, see relax below */
+#define GFD_RELAX_JACOBI 2  /* weighted Jacobi */
+
+typedef struct gfd_operator gfd_operator;
+typedef struct gfd_transformer gfd_transformer;
+typedef struct gfd_poisson gfd_poisson;
+
+/* Message of the last failing call on this thread ("" if none).  Returns the
+ * full message length; writes at most len-1 characters plus a NUL. */
+GFD_API size_t gfd_last_error(char* buf, size_t len);
+
+/* Library version string, e.g. "gpaw-fd-b200 0.1 sm_100a". */
+GFD_API const char* gfd_version(void);
+
+/* ------------------------------------------------------------------------
+ * Finite-difference operator.
+ * Replaces _gpaw.Operator(coefs, offsets, size, range, neighbors, real,
+ * comm, cfd) -- c/operators.c:465-498 -- whose Python caller is
+ * FDOperator.__init__ / allocate (gpaw/fd_operators.py:21-70).
+ *
+ *   ncoefs, coefs[ncoefs]  stencil weights (coefs[0] must be the diagonal
+ *                          for relax, as the reference assumes)
+ *   offsets[ncoefs*3]      integer (d0, d1, d2) offset of each weight.  The
+ *                          reference passes flat offsets on its padded grid;
+ *                          the padded grid does not exist here.
+ *   size[3]                points per axis (n_c)
+ *   range                  halo width (mp, the largest offset)
+ *   neighbors[6]           neighbor_cd as (axis, side): 0 = this domain
+ *                          (periodic wrap), -1 = none (zero boundary)
+ *   real                   1 for float arrays, 0 for complex (the reference
+ *                          builds one object per dtype)
+ *   cfd                    1 when no offset has two nonzero components
+ * ---------------------------------------------------------------------- */
+GFD_API int gfd_operator_create(int ncoefs, const double* coefs, const int64_t* offsets,
+                        const int64_t size[3], int range, const int64_t neighbors[6],
+                        int real, int cfd, gfd_operator** op);
+GFD_API int gfd_operator_destroy(gfd_operator* op);
+
+/* out[x] = sum_p coefs[p] * in[x + offsets[p]] for x in 0..nin-1, halos zero
+ * or periodic times phase_cd (Operator_apply, c/operators.c:316-405).
+ * phase_cd: 12 host doubles, phase_cd[c][d] as (re, im) at 4*c + 2*d, used
+ * for complex dtypes only (may be NULL: all phases 1).  The low halo on axis
+ * c takes phase_cd[c][1], the high halo phase_cd[c][0] (c/bc.c:234-249).
+ * in and out must not overlap. */
+GFD_API int gfd_operator_apply(gfd_operator* op, int dtype, const void* in, void* out, int64_t nin,
+                       const double* phase_cd, void* stream);
+
+/* nrelax sweeps of relaxation for "operator func = source", in place on
+ * func (Operator_relax, c/operators.c:49-91; bmgs_relax, c/bmgs/relax.c).
+ * Real dtypes only.  GFD_RELAX_JACOBI: weighted Jacobi with weight w, as
+ * the reference.  GFD_RELAX_GS: the reference's lexicographic Gauss-Seidel
+ * is a sequential sweep; it is replaced by multicolour Gauss-Seidel
+ * ((i0+i1+i2) mod (range+1) colours, a valid colouring for axis-aligned
+ * stencils), judged by the converged result, not by iterates.
+ * Uses a device scratch array of one grid owned by the operator. */
+GFD_API int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method, void* func,
+                       const void* source, int nrelax, double w, void* stream);
+
+/* Weight of the zero offset (Operator_get_diagonal_element,
+ * c/operators.c:408-421). */
+GFD_API int gfd_operator_get_diagonal_element(const gfd_operator* op, double* d);
+
+/* ------------------------------------------------------------------------
+ * Grid transformer (restriction / interpolation).
+ * Replaces _gpaw.Transformer(size_in, size_out, k, paddings, npaddings,
+ * skip, neighbors, real, comm, interpolate) -- c/transformers.c:222-265 --
+ * built by _Transformer (gpaw/transformers.py:19-79).  k = 2*nn in
+ * {2, 4, 6, 8}; pad/npad/skip/neighbors are [3][2] as (axis, side).
+ * ---------------------------------------------------------------------- */
+GFD_API int gfd_transformer_create(const int64_t size_in[3], const int64_t size_out[3], int k,
+                           const int64_t pad[6], const int64_t npad[6], const int64_t skip[6],
+                           const int64_t neighbors[6], int real, int interpolate,
+                           gfd_transformer** tr);
+GFD_API int gfd_transformer_destroy(gfd_transformer* tr);
+
+/* Transformer_apply (c/transformers.c:127-185): in has shape
+ * (nin, size_in), out (nin, size_out); phases as for gfd_operator_apply. */
+GFD_API int gfd_transformer_apply(gfd_transformer* tr, int dtype, const void* in, void* out,
+                          int64_t nin, const double* phases, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Multigrid Poisson solver (gpaw/poisson.py:21-276).
+ * Built from the level operators and transformers exactly as
+ * PoissonSolver.set_grid_descriptor builds them: ops[0..levels] with
+ * ops[0] the fine-grid Laplace (scale -1/(4 pi), nn) and ops[l>=1] nn=1;
+ * restrictors[l] / interpolators[l] between level l and l+1 (nn=1).
+ * presmooths/postsmooths/weights have levels+1 entries; the coarsest entry
+ * of presmooths/postsmooths is used as given (the reference sets it to 8).
+ * dv is the fine-grid volume element.  pbc_all is 1 when every axis is
+ * periodic (mean of phi removed after the solve).
+ * precision: GFD_POISSON_FP64 runs the V-cycle in float64 as the reference;
+ * GFD_POISSON_MIXED runs FP32 V-cycles inside an FP64 defect-correction
+ * loop (residual, update and norm in FP64).
+ * The solver allocates its level arrays on the device.
+ * ---------------------------------------------------------------------- */
+#define GFD_POISSON_FP64 0
+#define GFD_POISSON_MIXED 1
+
+GFD_API int gfd_poisson_create(int levels, gfd_operator* const* ops, gfd_transformer* const* restrictors,
+                       gfd_transformer* const* interpolators, const int* presmooths,
+                       const int* postsmooths, const double* weights, int relax_method,
+                       double dv, int pbc_all, int precision, gfd_poisson** ps);
+GFD_API int gfd_poisson_destroy(gfd_poisson* ps);
+
+/* PoissonSolver.solve(phi, rho, charge=None, eps, maxcharge) for a charge-
+ * neutral rho (gpaw/poisson.py:124-138, 193-218).  phi (in: initial guess,
+ * out: solution) and rho are device float64 arrays of the fine grid.
+ * charge: pass NaN for None (the integral of rho is used).  When
+ * |charge| > maxcharge the call returns GFD_EUNSUPPORTED (the charged
+ * branches are outside this library).  maxiter = 1000 in the reference.
+ * On return (the call waits for the stream) *niter holds the V-cycle count
+ * and *error the last residual norm sum(r^2) dv; GFD_ENOCONV when
+ * niter reached maxiter, as PoissonConvergenceError. */
+GFD_API int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho, double charge,
+                      double eps, double maxcharge, int maxiter, int* niter, double* error,
+                      void* stream);
+
+/* ------------------------------------------------------------------------
+ * Reductions.
+ * sum over all points of a float64 array of n elements, times scale (the
+ * integral of GridDescriptor.integrate, gpaw/grid_descriptor.py:197-215).
+ * Deterministic: a fixed reduction tree independent of timing.  Waits for
+ * the stream and writes the result to *result (host).
+ * ---------------------------------------------------------------------- */
+GFD_API int gfd_grid_sum(const double* a, int64_t n, double scale, double* result, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPAW_FD_H */

@@ -1,0 +1,164 @@
+"""Host-side logic and the C ABI, without a GPU.
+
+* libgpawfd.so loads and exports every function include/gpaw_fd.h declares;
+* handle constructors validate their arguments (host-only calls);
+* the product's coefficient builders, grid descriptor and transformer
+  paddings agree with the oracle's restatement of the reference.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import geometry as G
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, 'include', 'gpaw_fd.h')).read()
+    return sorted(set(re.findall(r'GFD_API\s+[\w\s\*]+?\b(gfd_\w+)\s*\(', text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from gpaw_b200 import _lib
+    names = header_functions()
+    assert len(names) >= 14
+    raw = ctypes.CDLL(_lib.LIB_PATH)
+    for name in names:
+        assert hasattr(raw, name), name
+    assert set(names) == set(_lib.SIGNATURES)
+    assert _lib.lib.gfd_version().startswith(b'gpaw-fd-b200')
+
+
+def _create_op(coefs, offsets, size, rng=None, nbr=None, real=1):
+    from gpaw_b200 import _lib
+    c, cp = _lib.f64(coefs)
+    o, op = _lib.i64(offsets)
+    s, sp = _lib.i64(size)
+    n, np_ = _lib.i64(nbr if nbr is not None else [-1] * 6)
+    h = _lib._vp()
+    mp = int(np.abs(np.asarray(offsets)).max())
+    st = _lib.lib.gfd_operator_create(len(c), cp, op, sp, mp if rng is None else rng, np_, real, 1,
+                                      ctypes.byref(h))
+    return st, h
+
+
+def test_operator_create_validates_arguments():
+    from gpaw_b200 import _lib
+    st, h = _create_op([-6.0, 1, 1, 1, 1, 1, 1],
+                       [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1),
+                        (0, 0, -1)], (8, 8, 8))
+    assert st == _lib.GFD_OK and h.value
+    d = ctypes.c_double()
+    assert _lib.lib.gfd_operator_get_diagonal_element(h, ctypes.byref(d)) == 0 and d.value == -6.0
+    assert _lib.lib.gfd_operator_destroy(h) == 0
+    # range smaller than the offsets
+    st, _ = _create_op([1.0, 1.0], [(0, 0, 0), (2, 0, 0)], (8, 8, 8), rng=1)
+    assert st == _lib.GFD_EINVAL and 'range' in _lib.last_error()
+    # periodic axis shorter than the halo
+    st, _ = _create_op([1.0, 1.0], [(0, 0, 0), (3, 0, 0)], (2, 8, 8), nbr=[0] * 6)
+    assert st == _lib.GFD_EINVAL
+    # another MPI rank as neighbour: no domain decomposition
+    st, _ = _create_op([1.0], [(0, 0, 0)], (8, 8, 8), nbr=[1, 1, -1, -1, -1, -1])
+    assert st == _lib.GFD_EUNSUPPORTED
+    # zero-size grid
+    st, _ = _create_op([1.0], [(0, 0, 0)], (0, 8, 8))
+    assert st == _lib.GFD_EINVAL
+
+
+def test_transformer_create_checks_sizes():
+    from gpaw_b200 import _lib
+    gd = G.Grid((16, 12, 20), (8.0, 6.0, 10.0), 0)
+    for g2 in (gd.coarsen(), gd.refine()):
+        for nn in (1, 2, 3):
+            pad, npad, skip, interp = G.transformer_layout(gd, g2, nn)
+            args = [_lib.i64(x) for x in (gd.n_c, g2.n_c, pad, npad, skip, gd.neighbor_cd)]
+            h = _lib._vp()
+            st = _lib.lib.gfd_transformer_create(args[0][1], args[1][1], 2 * nn, args[2][1],
+                                                 args[3][1], args[4][1], args[5][1], 1,
+                                                 int(interp), ctypes.byref(h))
+            assert st == 0, _lib.last_error()
+            _lib.lib.gfd_transformer_destroy(h)
+            # a wrong output size is rejected
+            bad = [_lib.i64(x) for x in (np.array(g2.n_c) + 1,)]
+            st = _lib.lib.gfd_transformer_create(args[0][1], bad[0][1], 2 * nn, args[2][1],
+                                                 args[3][1], args[4][1], args[5][1], 1,
+                                                 int(interp), ctypes.byref(h))
+            assert st == _lib.GFD_EINVAL
+
+
+CELLS = [((12, 12, 12), (3.6, 3.6, 3.6)),
+         ((8, 10, 12), (2.4, 3.0, 3.9)),
+         ((8, 8, 8), [(1, 0, 0), (0.5, 3 ** 0.5 / 2, 0), (0, 0, 1.1)]),
+         ((6, 6, 6), [(0, 1, 1), (1, 0, 1), (1, 1, 0)]),
+         ((6, 6, 6), [(-1, 1, 1), (1, -1, 1), (1, 1, -1)])]
+
+
+@pytest.mark.parametrize('N,cell', CELLS)
+def test_coefficients_match_oracle(N, cell):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.fd_operators import Gradient, Laplace
+    gd = GridDescriptor(N, cell, True)
+    og = G.Grid(N, cell, True)
+    for n in range(1, 7):
+        op = Laplace(gd, -0.5, n, allocate=False)
+        c, o = G.laplace_stencil(og, -0.5, n)
+        assert np.array_equal(op.offset_pc, o)
+        assert np.abs(op.coef_p - c).max() <= 1e-14 * np.abs(c).max()
+    for v in range(3):
+        for n in (1, 3, 5):
+            op = Gradient(gd, v, 1.0, n, allocate=False)
+            c, o = G.gradient_stencil(og, v, 1.0, n)
+            assert np.array_equal(op.offset_pc, o)
+            assert np.abs(op.coef_p - c).max() <= 1e-14 * np.abs(c).max()
+
+
+@pytest.mark.parametrize('pbc', [0, 1, (1, 0, 1)])
+def test_grid_descriptor_and_transformer_layout(pbc):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.transformers import Transformer
+    gd = GridDescriptor((16, 12, 20), (8.0, 6.0, 10.0), pbc)
+    og = G.Grid((16, 12, 20), (8.0, 6.0, 10.0), pbc)
+    for attr in ('n_c', 'beg_c', 'end_c', 'h_cv', 'neighbor_cd', 'sdisp_cd', 'xxxiucell_cv'):
+        assert np.allclose(getattr(gd, attr), getattr(og, attr), rtol=0, atol=0), attr
+    assert gd.dv == og.dv
+    assert np.array_equal(gd.get_size_of_global_array(), og.global_size())
+    for g2, o2 in ((gd.coarsen(), og.coarsen()), (gd.refine(), og.refine())):
+        for nn in (1, 2, 3, 4):
+            t = Transformer(gd, g2, nn, allocate=False)
+            pad, npad, skip, interp = G.transformer_layout(og, o2, nn)
+            assert np.array_equal(t.pad_cd, pad) and np.array_equal(t.neighborpad_cd, npad)
+            assert np.array_equal(t.skip_cd, skip) and t.interpolate == interp
+
+
+def test_poisson_hierarchy_matches_reference_rules():
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.poisson import PoissonSolver
+    from oracle.poisson import PoissonSolver as OraclePS
+    for N, pbc in ((128, 0), (48, 0), (20, 1), (6, 0)):
+        gd = GridDescriptor((N,) * 3, (N * 0.38,) * 3, pbc)
+        ps = PoissonSolver(nn=3)
+        ps.set_grid_descriptor(gd)
+        ops = OraclePS(3)
+        ops.set_grid_descriptor(G.Grid((N,) * 3, (N * 0.38,) * 3, pbc))
+        assert ps.levels == ops.levels
+        assert ps.presmooths == ops.presmooths and ps.postsmooths == ops.postsmooths
+        assert ps.weights == ops.weights
+        for a, (c, o) in zip(ps.operators, ops.stencils):
+            assert np.array_equal(a.offset_pc, o)
+            assert np.abs(a.coef_p - c).max() <= 1e-14 * np.abs(c).max()
+
+
+def test_no_cpu_path_for_host_tensors():
+    """Product calls reject host tensors instead of computing on the CPU."""
+    import torch
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.fd_operators import Laplace
+    gd = GridDescriptor((8, 8, 8), (2.0, 2.0, 2.0), 1, device='cpu')
+    op = Laplace(gd, -0.5, 2)
+    a = torch.zeros((8, 8, 8), dtype=torch.float64)
+    with pytest.raises(ValueError, match='CUDA'):
+        op.apply(a, torch.zeros_like(a))
