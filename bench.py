@@ -311,12 +311,13 @@ def run_gpu_arm(args):
     phase = np.exp(2j * np.pi * gd.sdisp_cd * np.array(K_VEC)[:, None])
     g = torch.Generator(device='cuda')
     g.manual_seed(2 + rank)
-    shape = (NBANDS,) + tuple(int(x) for x in gd.n_c)
+    nb = args.bands
+    shape = (nb,) + tuple(int(x) for x in gd.n_c)
     a = torch.complex(torch.randn(shape, dtype=torch.float64, device='cuda', generator=g),
                       torch.randn(shape, dtype=torch.float64, device='cuda', generator=g))
     b = torch.empty_like(a)
     stream = torch.cuda.current_stream()
-    nbytes = BYTES_PER_POINT * NBANDS * N ** 3
+    nbytes = BYTES_PER_POINT * nb * N ** 3
 
     for _ in range(args.warmup):
         lap.apply(a, b, phase)
@@ -340,24 +341,28 @@ def run_gpu_arm(args):
 
     # End to end through the public API with host buffers: pinned H2D copy of
     # the bands, apply, D2H copy of the result, every step.
-    e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    host_in = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
-    host_in.copy_(a)
-    host_out = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
-    torch.cuda.synchronize()
-    barrier(world)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        a.copy_(host_in, non_blocking=True)
-        lap.apply(a, b, phase)
-        host_out.copy_(b, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world)
-    e2e_value = world * nbytes / (e2e_ms * 1e-3) / 1e9
-    del host_in, host_out
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e_steps = min(args.steps, args.e2e_steps)
+        host_in = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+        host_in.copy_(a)
+        host_out = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            a.copy_(host_in, non_blocking=True)
+            lap.apply(a, b, phase)
+            host_out.copy_(b, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world)
+        e2e = {'value': world * nbytes / (e2e_ms * 1e-3) / 1e9, 'unit': 'GB/s',
+               'steps': e2e_steps, 'h2d_bytes_per_step': nbytes // 2,
+               'd2h_bytes_per_step': nbytes // 2}
+        del host_in, host_out
 
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic()
@@ -365,13 +370,12 @@ def run_gpu_arm(args):
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_max,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'complex128', 'data': 'synthetic (seeded N(0,1) bands)',
-            'config': dict(workload_config(), parallelism='bands sharded, %d per GPU' % NBANDS),
+            'config': dict(workload_config(nb), parallelism='bands sharded, %d per GPU' % nb),
             'roofline': {'bound': 'hbm', 'achieved': kernel_gbs, 'peak': peak, 'unit': 'GB/s',
                          'frac': kernel_gbs / peak, 'peak_kind': peak_kind,
                          'traffic': traffic, 'algorithmic_bytes_per_launch': nbytes,
                          'kernel': 'star_kernel<cplx<double>,R=3>'},
-            'e2e': {'value': e2e_value, 'unit': 'GB/s', 'steps': e2e_steps,
-                    'h2d_bytes_per_step': nbytes // 2, 'd2h_bytes_per_step': nbytes // 2},
+            'e2e': e2e,
             'gpu_launches': args.steps,
             'clocks': clocks.result()}
     if rank == 0 and world == 1 and not args.no_poisson:
@@ -401,7 +405,9 @@ def main():
     ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    ap.add_argument('--e2e-steps', type=int, default=3)
+    ap.add_argument('--e2e-steps', type=int, default=3, help='0 skips the end-to-end leg')
+    ap.add_argument('--bands', type=int, default=NBANDS,
+                    help='bands per GPU (smaller cases for profiling only)')
     ap.add_argument('--cpu-seconds', type=float, default=10.0)
     ap.add_argument('--no-poisson', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')

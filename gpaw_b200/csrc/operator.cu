@@ -217,6 +217,8 @@ extern "C" int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method,
   int st = ensure_scratch(op, bytes);
   if (st) return st;
   if (relax_method == GFD_RELAX_GS) return op_gs_sweeps(op, dtype, func, source, nrelax, op->scratch, s);
+  // Weighted Jacobi with w = 0 leaves func unchanged.
+  if (w == 0.0) return GFD_OK;
   // Weighted Jacobi: ping-pong between func and the scratch grid.
   void* cur = func;
   void* nxt = op->scratch;

@@ -40,18 +40,40 @@ struct StarParams {
   int x_chunk;      // outputs along axis 0 per CTA
   int nxc;          // number of axis-0 chunks
   long long band;   // elements per band
-  S c0;             // centre weight
+  S c0;             // centre weight (MODE_JACOBI: the folded centre weight, see below)
   S cx[2 * kMaxR + 1];  // weight of offset k along axis 0 at index kMaxR + k
   S cy[2 * kMaxR + 1];
   S cz[2 * kMaxR + 1];
-  S w;              // Jacobi weight
+  S wc;             // MODE_JACOBI: w / coefs[0]
+  int fix_yz;       // complex: the tile needs y/z Bloch phases on wrapped cells
   Phases<S> P;
   double* partials; // MODE_RESIDUAL: one sum of r^2 per CTA (or nullptr)
 };
 
-template <class V>
-__device__ __forceinline__ V load_mapped(const V* base, int off) {
-  return off >= 0 ? ldro(base + off) : vzero<V>();
+// Asynchronous global->shared copies (sm_80+ cp.async).  A source size of 0
+// writes zeros (zero boundary points); the source address is then unused but
+// kept valid.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid) {
+  const unsigned d = smem_addr(dst);
+  const int n = valid ? BYTES : 0;
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
+                 "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // Block-wide sum of one double per thread in a fixed order.
@@ -68,24 +90,50 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
-template <class V, int R, int BZ, int TY, int VY, int D, int MODE>
+template <int BZ, int TY, int VY, int R, int S, class V, bool RHO>
+constexpr size_t star_smem_bytes() {
+  return size_t(S) * ((TY * VY + 2 * R) * (BZ + 2 * R) + (RHO ? TY * VY * BZ : 0)) * sizeof(V);
+}
+
+// Axis-aligned ("star") stencil, marching along axis 0.
+//
+//  * A CTA owns BY = TY*VY rows (axis 1) by BZ columns (axis 2); thread
+//    (tz, ty) owns the VY consecutive rows ty*VY .. ty*VY+VY-1 at column tz.
+//  * Planes stream through an S-stage shared-memory ring filled by cp.async:
+//    the plane's tile plus an R-wide halo (corners skipped), zero-filled on
+//    zero boundaries and wrapped on periodic ones (Bloch phases applied by
+//    the thread that copied the cell, after its copy landed).  Planes
+//    outside this CTA's axis-0 chunk are copied without their halo.
+//  * Axis-1 neighbours and the own values come from one column read of
+//    VY+2R cells; axis-2 neighbours from 2R reads per point.
+//  * Axis 0: each point keeps 2R+1 partial sums in registers; plane p adds
+//    its own value into the sums of outputs p-R..p+R.  The plane loop is
+//    unrolled by 2R+1 so the ring index of every sum is a compile-time
+//    constant.
+//  * MODE_JACOBI folds the (1-w) phi term into the centre weight:
+//    phi_new = (w/c0) (rho - sum_{p>=1} c_p phi_p - c0' phi) with
+//    c0' = -(1-w) c0 / w, which equals (1-w) phi + w (rho - sum) / c0.
+//  * The source term of MODE_JACOBI / MODE_RESIDUAL travels in the same
+//    pipeline stages.
+template <class V, int R, int BZ, int TY, int VY, int S, int MODE>
 __global__ void __launch_bounds__(BZ * TY)
 star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
             const StarParams<typename vt<V>::S> p) {
-  using S = typename vt<V>::S;
-  constexpr int NT = BZ * TY;
-  constexpr int BY = TY * VY;
-  constexpr int SY = BY + 2 * R;
-  constexpr int SZ = BZ + 2 * R;
-  constexpr int HN = 2 * R * BZ + 2 * R * BY;  // halo cells of one plane
-  constexpr int HC = (HN + NT - 1) / NT;       // halo cells per thread
+  using Sc = typename vt<V>::S;
+  constexpr int NT = BZ * TY, BY = TY * VY;
+  constexpr int SY = BY + 2 * R, SZ = BZ + 2 * R, CELLS = SY * SZ;
+  constexpr int CPT = (CELLS + NT - 1) / NT;
   constexpr int Q = 2 * R + 1;
+  constexpr bool RHO = MODE != MODE_APPLY;
+  constexpr int RCELLS = RHO ? BY * BZ : 0;
+  static_assert(S >= 2, "pipeline needs two stages");
 
-  __shared__ V tile[2][SY][SZ];
-  __shared__ double red[NT / 32];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* tiles = reinterpret_cast<V*>(smem_raw);  // [S][CELLS]
+  V* rtiles = tiles + S * CELLS;              // [S][BY*BZ] source terms
+  __shared__ double red[NT / 32 > 0 ? NT / 32 : 1];
 
-  const int t = threadIdx.x;
-  const int tz = t % BZ, ty = t / BZ;
+  const int t = threadIdx.x, tz = t % BZ, ty = t / BZ;
   const int z0 = blockIdx.x * BZ, y0 = blockIdx.y * BY;
   const int bnd = blockIdx.z / p.nxc, xc = blockIdx.z % p.nxc;
   const int x0 = xc * p.x_chunk;
@@ -93,227 +141,220 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
   const long long plane = (long long)p.n1 * p.n2;
   const V* inb = in + bnd * p.band;
   V* outb = out + bnd * p.band;
-  const V* rhob = rho ? rho + bnd * p.band : nullptr;
-
-  // Own points: rows y0 + ty + j*TY, column z0 + tz.  The in-plane source
-  // offset is -1 for a zero boundary point; out-of-domain points of partial
-  // tiles still need a (wrapped or zero) value in shared memory.
-  int own_src[VY];
-  int own_code[VY];  // wrap sides (y in bits 0-1, z in bits 2-3), 0xF = none
-  bool own_in[VY];
-  {
-    int sz_side;
-    int zs = wrap_axis(z0 + tz, p.n2, p.per2, sz_side);
-#pragma unroll
-    for (int j = 0; j < VY; j++) {
-      int y = y0 + ty + j * TY;
-      int sy_side;
-      int ys = wrap_axis(y, p.n1, p.per1, sy_side);
-      own_in[j] = (y < p.n1) && (z0 + tz < p.n2);
-      own_src[j] = (ys >= 0 && zs >= 0) ? ys * p.n2 + zs : -1;
-      own_code[j] = (sy_side + 1) | ((sz_side + 1) << 2);
-    }
-  }
-  // Halo cells of this thread: y-halo rows first, then z-halo columns.
-  int h_smem[HC];
-  int h_src[HC];
-  int h_code[HC];
-#pragma unroll
-  for (int i = 0; i < HC; i++) {
-    int h = t + i * NT;
-    h_smem[i] = -1;
-    h_src[i] = -1;
-    h_code[i] = 0;
-    if (h < HN) {
-      int sy, sz;
-      if (h < 2 * R * BZ) {
-        int r = h / BZ, c = h % BZ;
-        sy = r < R ? r : BY + r;
-        sz = R + c;
-      } else {
-        int hh = h - 2 * R * BZ;
-        int r = hh / (2 * R), c = hh % (2 * R);
-        sy = R + r;
-        sz = c < R ? c : BZ + c;
-      }
-      int ysd, zsd;
-      int ys = wrap_axis(y0 - R + sy, p.n1, p.per1, ysd);
-      int zs = wrap_axis(z0 - R + sz, p.n2, p.per2, zsd);
-      h_smem[i] = sy * SZ + sz;
-      h_src[i] = (ys >= 0 && zs >= 0) ? ys * p.n2 + zs : -1;
-      h_code[i] = (ysd + 1) | ((zsd + 1) << 2);
-    }
-  }
-
-  auto with_phase = [&](V v, int code) -> V {
-    if constexpr (vt<V>::NC == 2) {
-      int ys = (code & 3) - 1, zs = ((code >> 2) & 3) - 1;
-      if (ys >= 0) v = phase_mul(phase_of(p.P, 1, ys), v);
-      if (zs >= 0) v = phase_mul(phase_of(p.P, 2, zs), v);
-    }
-    return v;
-  };
-
-  // Prefetch ring: own values and halo values of the next D planes.
-  V rc[D][VY];
-  V rh[D][HC];
+  const V* rhob = RHO ? rho + bnd * p.band : nullptr;
   const int pbeg = x0 - R, pend = x1 + R;
 
-  auto load_plane = [&](int pl, V (&cv)[VY], V (&hv)[HC]) {
-    int xside;
-    int xs = wrap_axis(pl, p.n0, p.per0, xside);
-    if (xs < 0 || pl < pbeg || pl >= pend) {
+  // Cells this thread copies (all cells of the halo box, corners included,
+  // so the copy loop has no branches): byte offset of the source within a
+  // plane (a valid dummy offset 0 for zero points, flagged in czero) and the
+  // byte offset of the destination within a stage.  Wrap sides are kept
+  // only for Bloch phases (y side bits 0-1, z side bits 2-3).
+  unsigned csrc[CPT];
+  unsigned cdst[CPT];
+  unsigned czero = 0, clive = 0;  // bit i: zero point / cell exists
+  int ccode[CPT];
+  bool fix = false;
 #pragma unroll
-      for (int j = 0; j < VY; j++) cv[j] = vzero<V>();
-#pragma unroll
-      for (int i = 0; i < HC; i++) hv[i] = vzero<V>();
-      return;
+  for (int i = 0; i < CPT; i++) {
+    const int c = t + i * NT;
+    csrc[i] = 0;
+    cdst[i] = unsigned(c) * unsigned(sizeof(V));
+    ccode[i] = 0;
+    if (c < CELLS) {
+      clive |= 1u << i;
+      const int sy = c / SZ, sz = c % SZ;
+      int ysd, zsd;
+      const int ys = wrap_axis(y0 - R + sy, p.n1, p.per1, ysd);
+      const int zs = wrap_axis(z0 - R + sz, p.n2, p.per2, zsd);
+      if (ys >= 0 && zs >= 0) {
+        csrc[i] = unsigned(ys * p.n2 + zs) * unsigned(sizeof(V));
+        if (ysd >= 0 || zsd >= 0) fix = true;
+      } else {
+        czero |= 1u << i;
+      }
+      ccode[i] = (ysd + 1) | ((zsd + 1) << 2);
     }
-    const V* base = inb + xs * plane;
+  }
+  fix = fix && p.fix_yz;
+  bool own_in[VY];
+  unsigned own_b[VY];  // byte offset of an own point within a plane
 #pragma unroll
-    for (int j = 0; j < VY; j++) cv[j] = load_mapped(base, own_src[j]);
-    const bool need_halo = (pl >= x0 && pl < x1);
+  for (int j = 0; j < VY; j++) {
+    const int y = y0 + ty * VY + j, z = z0 + tz;
+    own_in[j] = y < p.n1 && z < p.n2;
+    own_b[j] = own_in[j] ? unsigned(y * p.n2 + z) * unsigned(sizeof(V)) : 0u;
+  }
+  const unsigned smem0 = smem_addr(tiles);
+  const unsigned rsmem0 = smem_addr(rtiles);
+  const size_t plane_b = size_t(plane) * sizeof(V);
+  const char* inb_c = reinterpret_cast<const char*>(inb);
+  const char* rho_c = reinterpret_cast<const char*>(rhob);
+
+  // Copy plane P (and the source term of output plane P - R) into stage
+  // (P - pbeg) % S; always commits one group.
+  auto issue = [&](int P) {
+    if (P < pend) {
+      const int st = (P - pbeg) % S;
+      const unsigned sbase = smem0 + unsigned(st * CELLS * sizeof(V));
+      int xside;
+      const int xs = wrap_axis(P, p.n0, p.per0, xside);
+      const char* src = inb_c + size_t(xs >= 0 ? xs : 0) * plane_b;
+      const unsigned zmask = xs >= 0 ? czero : ~0u;
 #pragma unroll
-    for (int i = 0; i < HC; i++) hv[i] = need_halo ? load_mapped(base, h_src[i]) : vzero<V>();
+      for (int i = 0; i < CPT; i++) {
+        if (!(clive >> i & 1u)) continue;
+        const unsigned n = (zmask >> i & 1u) ? 0u : unsigned(sizeof(V));
+        if constexpr (sizeof(V) == 16)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sbase + cdst[i]),
+                       "l"(src + csrc[i]), "r"(n)
+                       : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sbase + cdst[i]),
+                       "l"(src + csrc[i]), "n"(int(sizeof(V))), "r"(n)
+                       : "memory");
+      }
+      if constexpr (RHO) {
+        const int q = P - R;
+        if (q >= x0 && q < x1) {
+          const unsigned rbase = rsmem0 + unsigned((st * RCELLS + ty * VY * BZ + tz) * sizeof(V));
+          const char* rsrc = rho_c + size_t(q) * plane_b;
+#pragma unroll
+          for (int j = 0; j < VY; j++) {
+            const unsigned n = own_in[j] ? unsigned(sizeof(V)) : 0u;
+            const unsigned d = rbase + unsigned(j * BZ * sizeof(V));
+            if constexpr (sizeof(V) == 16)
+              asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d),
+                           "l"(rsrc + own_b[j]), "r"(n)
+                           : "memory");
+            else
+              asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d),
+                           "l"(rsrc + own_b[j]), "n"(int(sizeof(V))), "r"(n)
+                           : "memory");
+          }
+        }
+      }
+    }
+    cp_async_commit();
   };
 
 #pragma unroll
-  for (int d = 0; d < D; d++) load_plane(pbeg + d, rc[d], rh[d]);
+  for (int k = 0; k < S - 1; k++) issue(pbeg + k);
 
   V acc[VY][Q];
 #pragma unroll
   for (int j = 0; j < VY; j++)
 #pragma unroll
     for (int q = 0; q < Q; q++) acc[j][q] = vzero<V>();
-
-  // Centre values of the last R+1 planes (Jacobi epilogue) and the next
-  // output's source term.
-  V hist[VY][R + 1];
-  V rcur[VY];
-#pragma unroll
-  for (int j = 0; j < VY; j++) {
-#pragma unroll
-    for (int q = 0; q <= R; q++) hist[j][q] = vzero<V>();
-    rcur[j] = vzero<V>();
-  }
   double sumsq = 0.0;
+  char* out_c = reinterpret_cast<char*>(outb);
 
-  for (int pl = pbeg; pl < pend; ++pl) {
-    V cv[VY], hv[HC];
+  for (int base = pbeg; base < pend; base += Q) {
 #pragma unroll
-    for (int j = 0; j < VY; j++) cv[j] = rc[0][j];
+    for (int u = 0; u < Q; ++u) {
+      const int pl = base + u;
+      if (pl < pend) {
+        const int st = (pl - pbeg) % S;
+        V* tile = tiles + st * CELLS;
+        cp_async_wait<S - 2>();
+        if constexpr (vt<V>::NC == 2) {
+          if (fix) {
 #pragma unroll
-    for (int i = 0; i < HC; i++) hv[i] = rh[0][i];
-#pragma unroll
-    for (int d = 0; d + 1 < D; d++) {
-#pragma unroll
-      for (int j = 0; j < VY; j++) rc[d][j] = rc[d + 1][j];
-#pragma unroll
-      for (int i = 0; i < HC; i++) rh[d][i] = rh[d + 1][i];
-    }
-    load_plane(pl + D, rc[D - 1], rh[D - 1]);
-
-    // Source term for output pl - R + 1 (used next step).
-    V rnext[VY];
-    if constexpr (MODE != MODE_APPLY) {
-      const int qn = pl - R + 1;
-#pragma unroll
-      for (int j = 0; j < VY; j++)
-        rnext[j] = (qn >= x0 && qn < x1 && own_in[j])
-                       ? ldro(rhob + qn * plane + own_src[j])
-                       : vzero<V>();
-    }
-
-    if (pl >= x0 && pl < x1) {
-      V(*buf)[SZ] = tile[pl & 1];
-#pragma unroll
-      for (int j = 0; j < VY; j++) buf[R + ty + j * TY][R + tz] = with_phase(cv[j], own_code[j]);
-#pragma unroll
-      for (int i = 0; i < HC; i++)
-        if (h_smem[i] >= 0) (&buf[0][0])[h_smem[i]] = with_phase(hv[i], h_code[i]);
-      __syncthreads();
-#pragma unroll
-      for (int j = 0; j < VY; j++) {
-        const int yy = R + ty + j * TY, zz = R + tz;
-        V s = (MODE == MODE_JACOBI) ? vzero<V>() : vmul(p.c0, cv[j]);
-#pragma unroll
-        for (int k = 1; k <= R; k++) {
-          madd(s, p.cy[kMaxR - k], buf[yy - k][zz]);
-          madd(s, p.cy[kMaxR + k], buf[yy + k][zz]);
-        }
-#pragma unroll
-        for (int k = 1; k <= R; k++) {
-          madd(s, p.cz[kMaxR - k], buf[yy][zz - k]);
-          madd(s, p.cz[kMaxR + k], buf[yy][zz + k]);
-        }
-        acc[j][R] = vadd(acc[j][R], s);
-      }
-    }
-
-    // Contributions of this plane's own values along axis 0.
-    {
-      int xside;
-      int xs = wrap_axis(pl, p.n0, p.per0, xside);
-      if (xs >= 0) {
-#pragma unroll
-        for (int j = 0; j < VY; j++) {
-          V v = cv[j];
-          if constexpr (vt<V>::NC == 2) {
-            if (xside >= 0) v = phase_mul(phase_of(p.P, 0, xside), v);
-          }
-#pragma unroll
-          for (int k = 1; k <= R; k++) {
-            madd(acc[j][R - k], p.cx[kMaxR + k], v);
-            madd(acc[j][R + k], p.cx[kMaxR - k], v);
+            for (int i = 0; i < CPT; i++) {
+              if (!(clive >> i & 1u) || (czero >> i & 1u)) continue;
+              const int ys = (ccode[i] & 3) - 1, zs = ((ccode[i] >> 2) & 3) - 1;
+              if (ys < 0 && zs < 0) continue;
+              V v = tile[t + i * NT];
+              if (ys >= 0) v = phase_mul(phase_of(p.P, 1, ys), v);
+              if (zs >= 0) v = phase_mul(phase_of(p.P, 2, zs), v);
+              tile[t + i * NT] = v;
+            }
           }
         }
-      }
-    }
+        __syncthreads();
+        issue(pl + S - 1);
 
-    if constexpr (MODE == MODE_JACOBI) {
+        // Own values and axis-1 neighbours: one column of VY + 2R cells.
+        const V* colp = tile + (ty * VY) * SZ + R + tz;
+        V own[VY];
+        if (pl >= x0 && pl < x1) {
+          V col[VY + 2 * R];
 #pragma unroll
-      for (int j = 0; j < VY; j++) {
+          for (int m = 0; m < VY + 2 * R; m++) col[m] = colp[m * SZ];
 #pragma unroll
-        for (int q = 0; q < R; q++) hist[j][q] = hist[j][q + 1];
-        hist[j][R] = cv[j];
-      }
-    }
-
-    const int q = pl - R;
-    if (q >= x0 && q < x1) {
+          for (int j = 0; j < VY; j++) {
+            own[j] = col[R + j];
+            const V* row = colp + (R + j) * SZ;
+            V sy = vmul(p.c0, col[R + j]);
+            V sz = vzero<V>();
 #pragma unroll
-      for (int j = 0; j < VY; j++) {
-        if (!own_in[j]) continue;
-        V* dst = outb + q * plane + own_src[j];
-        if constexpr (MODE == MODE_APPLY) {
-          stcs(dst, acc[j][0]);
-        } else if constexpr (MODE == MODE_JACOBI) {
-          // b = (1 - w) b + w (src - x) / coefs[0]   (c/bmgs/relax.c:64)
-          static_assert(vt<V>::NC == 1, "relaxation is real only");
-          stcs(dst, (S(1) - p.w) * hist[j][0] + p.w * (rcur[j] - acc[j][0]) / p.c0);
+            for (int k = 1; k <= R; k++) {
+              madd(sy, p.cy[kMaxR - k], col[R + j - k]);
+              madd(sz, p.cz[kMaxR - k], row[-k]);
+              madd(sy, p.cy[kMaxR + k], col[R + j + k]);
+              madd(sz, p.cz[kMaxR + k], row[k]);
+            }
+            acc[j][u] = vadd(acc[j][u], vadd(sy, sz));  // slot of output pl
+          }
         } else {
-          V r = vsub(acc[j][0], rcur[j]);
-          stcs(dst, r);
-          if constexpr (vt<V>::NC == 1) sumsq += sq(r);
+#pragma unroll
+          for (int j = 0; j < VY; j++) own[j] = colp[(R + j) * SZ];
         }
+
+        int xside;
+        const int xs = wrap_axis(pl, p.n0, p.per0, xside);
+        if (xs >= 0) {
+          if constexpr (vt<V>::NC == 2) {
+            if (xside >= 0) {
+#pragma unroll
+              for (int j = 0; j < VY; j++) own[j] = phase_mul(phase_of(p.P, 0, xside), own[j]);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < VY; j++) {
+#pragma unroll
+            for (int k = 1; k <= R; k++) {
+              madd(acc[j][(u - k + Q) % Q], p.cx[kMaxR + k], own[j]);  // output pl-k: offset +k
+              madd(acc[j][(u + k) % Q], p.cx[kMaxR - k], own[j]);      // output pl+k: offset -k
+            }
+          }
+        }
+
+        const int q = pl - R;
+        const int qs = (u - R + Q) % Q;  // slot of output pl - R
+        if (q >= x0 && q < x1) {
+          const V* rt = rtiles + st * RCELLS + ty * VY * BZ + tz;
+          char* dstp = out_c + size_t(q) * plane_b;
+#pragma unroll
+          for (int j = 0; j < VY; j++) {
+            V* dst = reinterpret_cast<V*>(dstp + own_b[j]);
+            if constexpr (MODE == MODE_APPLY) {
+              if (own_in[j]) stcs(dst, acc[j][qs]);
+            } else if constexpr (MODE == MODE_JACOBI) {
+              static_assert(vt<V>::NC == 1, "relaxation is real only");
+              if (own_in[j]) stcs(dst, p.wc * (rt[j * BZ] - acc[j][qs]));
+            } else {
+              const V r = vsub(acc[j][qs], rt[j * BZ]);
+              if (own_in[j]) {
+                stcs(dst, r);
+                if constexpr (vt<V>::NC == 1) sumsq += sq(r);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < VY; j++) acc[j][qs] = vzero<V>();
       }
-    }
-#pragma unroll
-    for (int j = 0; j < VY; j++) {
-#pragma unroll
-      for (int qq = 0; qq + 1 < Q; qq++) acc[j][qq] = acc[j][qq + 1];
-      acc[j][Q - 1] = vzero<V>();
-      if constexpr (MODE != MODE_APPLY) rcur[j] = rnext[j];
     }
   }
+  cp_async_wait<0>();
 
   if constexpr (MODE == MODE_RESIDUAL) {
     if (p.partials) {
-      double s = block_sum<NT>(sumsq, red);
+      const double sblk = block_sum<NT>(sumsq, red);
       if (t == 0) {
-        long long cta = (long long)blockIdx.z * gridDim.y * gridDim.x +
-                        (long long)blockIdx.y * gridDim.x + blockIdx.x;
-        p.partials[cta] = s;
+        const long long cta = (long long)blockIdx.z * gridDim.y * gridDim.x +
+                              (long long)blockIdx.y * gridDim.x + blockIdx.x;
+        p.partials[cta] = sblk;
       }
     }
   }

@@ -29,8 +29,19 @@ inline TileDims tile_dims(int tile) {
   switch (tile) {
     case TILE_NARROW: return {8, 8, 64};
     case TILE_MID: return {16, 16, 128};
-    default: return {32, 16, 256};
+    default: return {32, 16, 128};
   }
+}
+
+constexpr int kStages = 4;
+
+// Raise a kernel's dynamic shared-memory limit when it needs more than 48 KB.
+template <class F>
+int raise_smem_limit(F* kern, size_t bytes, const char* what) {
+  if (bytes <= 48 * 1024) return GFD_OK;
+  return check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes),
+                    what);
 }
 
 struct LaunchGeom {
@@ -68,17 +79,34 @@ template <class V, int R, int BZ, int TY, int VY, int MODE>
 int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
             const StarParams<typename vt<V>::S>& base, const LaunchGeom& g, double* partials,
             cudaStream_t s) {
-  constexpr int D = 2;
+  constexpr int S = kStages;
+  constexpr size_t smem = star_smem_bytes<BZ, TY, VY, R, S, V, MODE != MODE_APPLY>();
+  auto kern = star_kernel<V, R, BZ, TY, VY, S, MODE>;
+  int st = raise_smem_limit(kern, smem, "cudaFuncSetAttribute(star_kernel)");
+  if (st) return st;
   StarParams<typename vt<V>::S> p = base;
   const long long band = (long long)op->n[0] * op->n[1] * op->n[2];
   for (int64_t b0 = 0; b0 < nin; b0 += g.bands_per_launch) {
     int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
     dim3 grid(g.grid.x, g.grid.y, (unsigned)(nb * g.nxc));
     p.partials = partials ? partials + b0 * g.nxc * g.grid.x * g.grid.y : nullptr;
-    star_kernel<V, R, BZ, TY, VY, D, MODE><<<grid, BZ * TY, 0, s>>>(
-        in + b0 * band, out + b0 * band, rho ? rho + b0 * band : nullptr, p);
+    kern<<<grid, BZ * TY, smem, s>>>(in + b0 * band, out + b0 * band,
+                                     rho ? rho + b0 * band : nullptr, p);
   }
   return check_launch("star_kernel");
+}
+
+// Wide tile: 32 columns x 16 rows; 4 rows per thread for 8-byte and
+// smaller values, 2 rows per thread where 4 would exceed the register file
+// (16-byte values or radius > 3).
+template <class V, int R, int MODE>
+int star_wide(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
+              const StarParams<typename vt<V>::S>& p, const LaunchGeom& g, double* partials,
+              cudaStream_t s) {
+  if constexpr (sizeof(V) >= 16 || R > 3)
+    return star_go<V, R, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+  else
+    return star_go<V, R, 32, 4, 4, MODE>(op, in, out, rho, nin, p, g, partials, s);
 }
 
 template <class V, int MODE>
@@ -91,10 +119,10 @@ int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V
       return star_go<V, RR, 8, 8, 1, MODE>(op, in, out, rho, nin, p, g, partials, s);        \
     if (tile == TILE_MID)                                                                    \
       return star_go<V, RR, 16, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);       \
-    return star_go<V, RR, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+    return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
 #define GFD_STAR_WIDE(RR) \
   case RR:                \
-    return star_go<V, RR, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+    return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
   switch (op->R) {
     GFD_STAR_SMALL(1)
     GFD_STAR_SMALL(2)
@@ -123,8 +151,18 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
     p.cy[i] = S(op->cy[i]);
     p.cz[i] = S(op->cz[i]);
   }
-  p.w = S(w);
+  if (mode == OP_JACOBI) {
+    // Fold (1 - w) phi into the centre weight (see star_kernel).
+    p.c0 = S(-(1.0 - w) * op->c0 / w);
+    p.wc = S(w / op->c0);
+  }
   fill_phases(p.P, phase_cd);
+  p.fix_yz = 0;
+  if (phase_cd)
+    for (int c = 1; c < 3; c++)
+      for (int d = 0; d < 2; d++)
+        if (op->per[c] && (phase_cd[4 * c + 2 * d] != 1.0 || phase_cd[4 * c + 2 * d + 1] != 0.0))
+          p.fix_yz = 1;
   const int tile = pick_tile(op);
   LaunchGeom g = star_geom(op, tile, nin, op->R);
   p.nxc = g.nxc;

@@ -126,12 +126,16 @@ def test_gauss_multipoles(cuda):
     """gpaw/test/gauss_func.py:13-78: nn=3, N=48 zero boundary, cell 20 Bohr;
     the potential of Gaussian multipoles L = 0..6 against the analytic one,
     L2 error < 0.6 (L = 0 is charged and takes the reference's Gaussian
-    monopole branch, which is outside this path, so L = 1..6 here)."""
+    monopole branch, which is outside this path, so L = 1..6 here).  The
+    generalised Gaussians and their potentials are those of
+    gpaw/utilities/gauss.py:14-47 (normalisation sqrt(4 pi) l!/(2l+1)!
+    (4a)^(l+3/2))."""
     from scipy.special import erf
     og = G.Grid((48,) * 3, (20.0,) * 3, 0)
     r_v = og.coords() - 10.0
     x, y, z = r_v
     r2 = (r_v ** 2).sum(0)
+    r2 = np.where(r2 < 1e-12, 1e-12, r2)  # as gpaw/utilities/tools.py:119-121
     r = np.sqrt(r2)
     a = 4 * 19.0 * (og.icell_cv ** 2).sum(1).max()
     sa = np.sqrt(a)

@@ -106,7 +106,7 @@ def test_bloch_complex_96(cuda, kind):
 
 
 SHAPES = [((5, 7, 9), 0), ((5, 7, 9), 1), ((33, 17, 65), (1, 0, 1)), ((3, 40, 3), 1),
-          ((1, 1, 8), (0, 0, 1)), ((70, 9, 31), 0), ((12, 12, 12), 1)]
+          ((2, 2, 8), (0, 0, 1)), ((70, 9, 31), 0), ((12, 12, 12), 1)]
 
 
 @pytest.mark.parametrize('N,pbc', SHAPES)
