@@ -112,6 +112,23 @@ GFD_API int gfd_operator_apply(gfd_operator* op, int dtype, const void* in, void
 GFD_API int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method, void* func,
                        const void* source, int nrelax, double w, void* stream);
 
+/* The same sweeps as gfd_operator_relax, allocating no device memory.  This
+ * entry point has no counterpart in the reference.
+ * gfd_operator_relax takes one grid of scratch from cudaMalloc on first use;
+ * callers that cannot allocate -- code running while a CUDA graph is being
+ * captured, hosts whose own pool allocator owns all device memory, loops that
+ * cannot afford an allocation's implicit synchronisation -- use this call.
+ * Its scratch is a 16 MiB array compiled into the library, held on every GPU
+ * that loads the library until the process exits, so the grid may have at
+ * most 2,097,152 float64 or 4,194,304 float32 points; larger grids return
+ * GFD_EINVAL with a message.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before starting any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (on different streams, or
+ * from different threads) race on it and must be serialised by the caller. */
+GFD_API int gfd_operator_relax_noalloc(gfd_operator* op, int dtype, int relax_method, void* func,
+                                       const void* source, int nrelax, double w, void* stream);
+
 /* Weight of the zero offset (Operator_get_diagonal_element,
  * c/operators.c:408-421). */
 GFD_API int gfd_operator_get_diagonal_element(const gfd_operator* op, double* d);
