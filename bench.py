@@ -411,9 +411,18 @@ def main():
     ap.add_argument('--cpu-seconds', type=float, default=10.0)
     ap.add_argument('--no-poisson', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--only', choices=['poisson'], default=None,
+                    help='run only the Poisson solves/s sub-benchmark (profiling)')
+    ap.add_argument('--solves', type=int, default=8, help='timed solves per precision')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference_arm(args)
+    if args.only == 'poisson':
+        import torch
+        torch.cuda.set_device(0)
+        pb, _, _, _ = poisson_bench(args.solves)
+        print(json.dumps({'poisson': pb}))
+        return 0
     return run_gpu_arm(args)
 
 

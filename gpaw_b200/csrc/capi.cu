@@ -1,6 +1,7 @@
 // capi.cu -- error reporting, device queries, reductions and small streaming
 // launches of libgpawfd.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -29,6 +30,25 @@ int check_cuda(cudaError_t e, const char* what) {
 
 int check_launch(const char* what) { return check_cuda(cudaGetLastError(), what); }
 
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("GFD_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+int zero_launch(int dtype, void* y, int64_t n, cudaStream_t s) {
+  const int blocks = grid_for(n);
+  if (dtype == GFD_FLOAT64)
+    launch_k(zero_kernel<double>, blocks, 256, 0, s, static_cast<double*>(y), (long long)n);
+  else if (dtype == GFD_FLOAT32)
+    launch_k(zero_kernel<float>, blocks, 256, 0, s, static_cast<float*>(y), (long long)n);
+  else
+    return set_error(GFD_EINVAL, "zero: unsupported dtype");
+  return check_launch("zero_kernel");
+}
+
 int num_sms() {
   static int cache[64] = {0};
   int dev = 0;
@@ -46,28 +66,28 @@ int reduce_launch(int dtype, const void* a, int64_t n, bool square, double scale
                   double* partials, double* result, cudaStream_t s) {
   if (dtype == GFD_FLOAT64) {
     if (square)
-      partial_sum_kernel<double, true><<<kRedBlocks, kRedThreads, 0, s>>>(
+      launch_k(partial_sum_kernel<double, true>, kRedBlocks, kRedThreads, 0, s, 
           static_cast<const double*>(a), n, partials);
     else
-      partial_sum_kernel<double, false><<<kRedBlocks, kRedThreads, 0, s>>>(
+      launch_k(partial_sum_kernel<double, false>, kRedBlocks, kRedThreads, 0, s, 
           static_cast<const double*>(a), n, partials);
   } else if (dtype == GFD_FLOAT32) {
     if (square)
-      partial_sum_kernel<float, true><<<kRedBlocks, kRedThreads, 0, s>>>(
+      launch_k(partial_sum_kernel<float, true>, kRedBlocks, kRedThreads, 0, s, 
           static_cast<const float*>(a), n, partials);
     else
-      partial_sum_kernel<float, false><<<kRedBlocks, kRedThreads, 0, s>>>(
+      launch_k(partial_sum_kernel<float, false>, kRedBlocks, kRedThreads, 0, s, 
           static_cast<const float*>(a), n, partials);
   } else {
     return set_error(GFD_EINVAL, "reductions need a real dtype");
   }
-  final_sum_kernel<<<1, kRedThreads, 0, s>>>(partials, kRedBlocks, scale, result);
+  launch_k(final_sum_kernel, 1, kRedThreads, 0, s, partials, kRedBlocks, scale, result);
   return check_launch("partial_sum_kernel");
 }
 
 int final_sum_launch(const double* partials, int n, double scale, double* result,
                      cudaStream_t s) {
-  final_sum_kernel<<<1, kRedThreads, 0, s>>>(partials, n, scale, result);
+  launch_k(final_sum_kernel, 1, kRedThreads, 0, s, partials, n, scale, result);
   return check_launch("final_sum_kernel");
 }
 
@@ -75,13 +95,13 @@ int axpby_launch(int ydtype, void* y, int xdtype, const void* x, double a, doubl
                  cudaStream_t s) {
   const int blocks = grid_for(n);
   if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT64)
-    axpby_kernel<double, double><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+    launch_k(axpby_kernel<double, double>, blocks, 256, 0, s, static_cast<double*>(y),
                                                         static_cast<const double*>(x), a, b, n);
   else if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT32)
-    axpby_kernel<double, float><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+    launch_k(axpby_kernel<double, float>, blocks, 256, 0, s, static_cast<double*>(y),
                                                        static_cast<const float*>(x), a, b, n);
   else if (ydtype == GFD_FLOAT32 && xdtype == GFD_FLOAT32)
-    axpby_kernel<float, float><<<blocks, 256, 0, s>>>(static_cast<float*>(y),
+    launch_k(axpby_kernel<float, float>, blocks, 256, 0, s, static_cast<float*>(y),
                                                       static_cast<const float*>(x), a, b, n);
   else
     return set_error(GFD_EINVAL, "axpby: unsupported dtype pair");
@@ -91,10 +111,10 @@ int axpby_launch(int ydtype, void* y, int xdtype, const void* x, double a, doubl
 int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cudaStream_t s) {
   const int blocks = grid_for(n);
   if (dtype == GFD_FLOAT64)
-    sub_const_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+    launch_k(sub_const_kernel<double>, blocks, 256, 0, s, static_cast<double*>(y),
                                                     static_cast<const double*>(x), c, n);
   else if (dtype == GFD_FLOAT32)
-    sub_const_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(y),
+    launch_k(sub_const_kernel<float>, blocks, 256, 0, s, static_cast<float*>(y),
                                                    static_cast<const float*>(x), c, n);
   else
     return set_error(GFD_EINVAL, "sub_const: unsupported dtype");
@@ -104,10 +124,10 @@ int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cud
 int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s) {
   const int blocks = grid_for(n);
   if (ydtype == GFD_FLOAT32 && xdtype == GFD_FLOAT64)
-    convert_kernel<float, double><<<blocks, 256, 0, s>>>(static_cast<float*>(y),
+    launch_k(convert_kernel<float, double>, blocks, 256, 0, s, static_cast<float*>(y),
                                                          static_cast<const double*>(x), n);
   else if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT32)
-    convert_kernel<double, float><<<blocks, 256, 0, s>>>(static_cast<double*>(y),
+    launch_k(convert_kernel<double, float>, blocks, 256, 0, s, static_cast<double*>(y),
                                                          static_cast<const float*>(x), n);
   else
     return set_error(GFD_EINVAL, "convert: unsupported dtype pair");

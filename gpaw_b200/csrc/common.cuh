@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <utility>
 
 #include "gpaw_fd.h"
 
@@ -121,6 +122,39 @@ struct Phases {
 template <class S>
 __device__ __forceinline__ cplx<S> phase_of(const Phases<S>& P, int c, int side) {
   return P.ph[c][side];
+}
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch.  Every kernel of the library starts with
+// pdl_enter(): it lets the next kernel on the stream be scheduled at once
+// (so its launch overlaps this one), then waits until the previous kernel
+// has completed and its writes are visible.  All global reads and writes
+// come after the wait, so a dependent kernel never sees a predecessor's
+// partial results.  Both instructions are no-ops for a normal launch.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
+bool pdl_enabled();
+
+// Launch with the programmatic-stream-serialisation attribute (when
+// enabled; GFD_PDL=0 in the environment turns it off).
+template <class... P, class... A>
+inline cudaError_t launch_k(void (*kern)(P...), dim3 grid, dim3 block, size_t smem,
+                            cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
 }
 
 // ---------------------------------------------------------------------------

@@ -64,6 +64,10 @@ int op_gs_colors(const gfd_operator* op);
 
 int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,
               const double* phases, cudaStream_t s);
+// Interpolation with the correction fused: out = base - interpolate(in)
+// (in place when base == out).
+int tr_launch_sub(const gfd_transformer* tr, int dtype, const void* in, void* out,
+                  const void* base, int64_t nin, const double* phases, cudaStream_t s);
 
 // Deterministic sum of n elements (float64 or float32 by dtype), SQUARE for
 // the sum of squares; result (device) = scale * sum.  partials needs
@@ -76,5 +80,6 @@ int axpby_launch(int ydtype, void* y, int xdtype, const void* x, double a, doubl
                  cudaStream_t s);
 int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cudaStream_t s);
 int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s);
+int zero_launch(int dtype, void* y, int64_t n, cudaStream_t s);
 
 }  // namespace gfd

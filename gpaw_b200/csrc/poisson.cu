@@ -6,7 +6,17 @@
 //   phi_{l+1} = 0; iterate2(l+1); phi_l -= interpolate(phi_{l+1});
 // then relax(postsmooths[l]) and, on level 0, the residual norm
 // sum(r^2) dv.  Weighted Jacobi sweeps ping-pong between two buffers per
-// level, so no copy is needed between sweeps.
+// level.  On level 0 the correction phi -= interpolate(e) is written out of
+// place (into the other buffer), so with 2 + 1 sweeps every V-cycle starts
+// and ends in the same buffer; the coarser levels do an even number of
+// sweeps and correct in place.
+//
+// A whole solve is one CUDA graph launch: the charge reduction, background
+// subtraction and a `while` conditional node whose body is one V-cycle, the
+// residual norm and a one-thread kernel applying the reference's stopping
+// rule (gpaw/poisson.py:203-204) on the device.  The graph is captured on the
+// first solve and reused; the caller's phi and rho are copied in and out
+// around it, and the host waits once per solve.
 //
 // GFD_POISSON_MIXED: defect correction.  The V-cycle is a linear iteration
 // phi <- phi + B (rho - L phi), so running it in float32 on the defect
@@ -15,6 +25,8 @@
 // the residual, the update and the norm stay float64.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
+#include <cstdlib>
 #include <new>
 #include <string>
 #include <vector>
@@ -28,13 +40,66 @@ namespace {
 struct Level {
   gfd_operator* op = nullptr;
   int64_t n = 0;
-  void* phi[2] = {nullptr, nullptr};  // level 0 (FP64 form): phi[0] is the caller's array
-  int cur = 0;
+  void* phi[2] = {nullptr, nullptr};
   void* rho = nullptr;
   void* res = nullptr;
   int pre = 0, post = 0;
   double w = 1.0;
 };
+
+// Solve controls shared by host and device.  The host writes the inputs
+// before each launch and reads the outputs after it.
+struct SolveCtrl {
+  double eps;
+  double maxcharge;
+  double charge_arg;  // NaN: use the integral of rho
+  int maxiter;
+  int pad0;
+  double charge;      // integral of rho times dv
+  double bg;          // background charge density removed from rho
+  double err;         // last residual norm sum(r^2) dv
+  double sum;         // scratch scalar (sum of phi)
+  int niter;
+  int status;         // GFD_OK or GFD_EUNSUPPORTED (charged)
+};
+
+__global__ void prep_kernel(SolveCtrl* c, double npoints, double dv,
+                            cudaGraphConditionalHandle loop, int in_graph) {
+  gfd::pdl_enter();
+  c->bg = c->charge / dv / npoints;
+  const double q = isnan(c->charge_arg) ? c->charge : c->charge_arg;
+  c->status = fabs(q) > c->maxcharge ? GFD_EUNSUPPORTED : GFD_OK;
+  c->niter = 0;
+  c->err = 0.0;
+  if (c->status != GFD_OK && in_graph) cudaGraphSetConditional(loop, 0);
+}
+
+// One V-cycle done: count it and decide whether to run another
+// (while iterate2() > eps and niter < maxiter).  in_graph = 0 (eager mode):
+// only count; the host applies the rule.
+__global__ void check_kernel(SolveCtrl* c, cudaGraphConditionalHandle loop, int in_graph) {
+  gfd::pdl_enter();
+  const int n = ++c->niter;
+  if (in_graph) cudaGraphSetConditional(loop, (c->err > c->eps && n < c->maxiter) ? 1u : 0u);
+}
+
+// y = x - bg (background removal), bg read from the controls.
+__global__ void __launch_bounds__(256) sub_bg_kernel(double* y, const double* x,
+                                                     const SolveCtrl* c, long long n) {
+  gfd::pdl_enter();
+  const double bg = c->bg;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+    y[i] = x[i] - bg;
+}
+
+// phi -= sum / n (zero mean potential in fully periodic systems).
+__global__ void __launch_bounds__(256) sub_mean_kernel(double* phi, const SolveCtrl* c,
+                                                       long long n) {
+  gfd::pdl_enter();
+  const double m = c->sum / double(n);
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+    phi[i] -= m;
+}
 
 }  // namespace
 
@@ -47,70 +112,265 @@ struct gfd_poisson {
   int precision = GFD_POISSON_FP64;
   std::vector<Level> L;     // hierarchy in the V-cycle precision
   int vdtype = GFD_FLOAT64; // dtype of the V-cycle arrays
-  // Mixed form: float64 fine-grid residual and alternate phi.
-  void* r64 = nullptr;
-  void* phi64_alt = nullptr;
+  // Float64 fine-grid arrays: the caller's rho and phi are copied here.
+  double* rho_in = nullptr;
+  double* phi64 = nullptr;  // mixed form: the float64 potential
+  double* rho64 = nullptr;  // mixed form: rho - background
+  double* r64 = nullptr;    // mixed form: float64 residual
   double* partials = nullptr;
   int64_t npartials = 0;
-  double* dscal = nullptr;  // device scalars: [0] err, [1] sum
-  double* hscal = nullptr;  // pinned host mirror
+  SolveCtrl* dctrl = nullptr;
+  SolveCtrl* hctrl = nullptr;  // pinned
   void* pool = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = -1;
 };
 
 namespace gfd {
 
-static int relax_level(gfd_poisson* ps, Level& lv, int nsweeps, cudaStream_t s) {
+static int relax_level(gfd_poisson* ps, Level& lv, int& cur, int nsweeps, cudaStream_t s) {
   if (nsweeps <= 0) return GFD_OK;
   if (ps->relax_method == GFD_RELAX_GS)
-    return op_gs_sweeps(lv.op, ps->vdtype, lv.phi[lv.cur], lv.rho, nsweeps, lv.phi[1 - lv.cur], s);
+    return op_gs_sweeps(lv.op, ps->vdtype, lv.phi[cur], lv.rho, nsweeps, lv.phi[1 - cur], s);
   for (int k = 0; k < nsweeps; k++) {
-    int st = op_launch(lv.op, ps->vdtype, OP_JACOBI, lv.phi[lv.cur], lv.phi[1 - lv.cur], lv.rho, 1,
+    int st = op_launch(lv.op, ps->vdtype, OP_JACOBI, lv.phi[cur], lv.phi[1 - cur], lv.rho, 1,
                        nullptr, lv.w, nullptr, s);
     if (st) return st;
-    lv.cur = 1 - lv.cur;
+    cur = 1 - cur;
   }
   return GFD_OK;
 }
 
-// One V-cycle from level l down.  final_norm: compute the level-0 residual
-// norm into dscal[0] (FP64 form only).
+// Enqueue one V-cycle from level l down; every level starts in phi[0] and
+// ends there.  final_norm: the level-0 residual norm into dctrl->err.
 static int iterate2(gfd_poisson* ps, int l, bool final_norm, cudaStream_t s) {
   Level& lv = ps->L[l];
   const size_t esz = dtype_size(ps->vdtype);
+  int cur = 0;
   int st;
   if (l < ps->levels) {
     Level& nx = ps->L[l + 1];
-    if ((st = relax_level(ps, lv, lv.pre, s))) return st;
-    if ((st = op_launch(lv.op, ps->vdtype, OP_RESIDUAL, lv.phi[lv.cur], lv.res, lv.rho, 1, nullptr,
+    if ((st = relax_level(ps, lv, cur, lv.pre, s))) return st;
+    if ((st = op_launch(lv.op, ps->vdtype, OP_RESIDUAL, lv.phi[cur], lv.res, lv.rho, 1, nullptr,
                         0.0, nullptr, s)))
       return st;
     if ((st = tr_launch(ps->restr[l], ps->vdtype, lv.res, nx.rho, 1, nullptr, s))) return st;
-    if ((st = check_cuda(cudaMemsetAsync(nx.phi[nx.cur], 0, nx.n * esz, s), "cudaMemsetAsync")))
-      return st;
+    if ((st = zero_launch(ps->vdtype, nx.phi[0], nx.n, s))) return st;
     if ((st = iterate2(ps, l + 1, false, s))) return st;
-    if ((st = tr_launch(ps->interp[l], ps->vdtype, nx.phi[nx.cur], lv.res, 1, nullptr, s)))
+    // phi -= interpolate(e): out of place when the sweeps left level l in an
+    // odd position, so the post-smoothing ends in phi[0].
+    const bool flip = ((lv.post & 1) != 0) != (cur != 0) && ps->relax_method != GFD_RELAX_GS;
+    const int dst = flip ? 1 - cur : cur;
+    if ((st = tr_launch_sub(ps->interp[l], ps->vdtype, nx.phi[0], lv.phi[dst], lv.phi[cur], 1,
+                            nullptr, s)))
       return st;
-    if ((st = axpby_launch(ps->vdtype, lv.phi[lv.cur], ps->vdtype, lv.res, 1.0, -1.0, lv.n, s)))
+    cur = dst;
+  }
+  if ((st = relax_level(ps, lv, cur, lv.post, s))) return st;
+  if (cur != 0) {
+    // Only reachable for an odd total sweep count on a level without the
+    // flip (possible with custom smoothing counts): copy back to phi[0].
+    if ((st = check_cuda(cudaMemcpyAsync(lv.phi[0], lv.phi[cur], lv.n * esz,
+                                         cudaMemcpyDeviceToDevice, s),
+                         "cudaMemcpyAsync(phi)")))
       return st;
   }
-  if ((st = relax_level(ps, lv, lv.post, s))) return st;
   if (l == 0 && final_norm) {
-    if ((st = op_launch(lv.op, ps->vdtype, OP_RESIDUAL, lv.phi[lv.cur], lv.res, lv.rho, 1, nullptr,
-                        0.0, ps->partials, s)))
+    if ((st = op_launch(lv.op, ps->vdtype, OP_RESIDUAL, lv.phi[0], lv.res, lv.rho, 1, nullptr, 0.0,
+                        ps->partials, s)))
       return st;
-    if ((st = final_sum_launch(ps->partials, (int)ps->npartials, ps->dv, ps->dscal, s))) return st;
+    if ((st = final_sum_launch(ps->partials,
+                               (int)op_partials(lv.op, GFD_FLOAT64, OP_RESIDUAL, 1), ps->dv,
+                               &ps->dctrl->err, s)))
+      return st;
   }
   return GFD_OK;
 }
 
-static int read_scalar(gfd_poisson* ps, int idx, double* out, cudaStream_t s) {
-  int st = check_cuda(cudaMemcpyAsync(ps->hscal + idx, ps->dscal + idx, sizeof(double),
-                                      cudaMemcpyDeviceToHost, s),
-                      "cudaMemcpyAsync(scalar)");
+// Body of the solve loop: one iteration of the chosen form, ending with the
+// stopping-rule kernel.
+static int loop_body(gfd_poisson* ps, cudaGraphConditionalHandle loop, int in_graph,
+                     cudaStream_t s) {
+  int st;
+  Level& L0 = ps->L[0];
+  const int64_t n0 = L0.n;
+  if (ps->precision == GFD_POISSON_FP64) {
+    if ((st = iterate2(ps, 0, true, s))) return st;
+  } else {
+    // rho_V = float(L phi - rho); e = 0; one float32 V-cycle; phi -= e;
+    // r = L phi - rho with its norm.
+    if ((st = convert_launch(GFD_FLOAT32, L0.rho, GFD_FLOAT64, ps->r64, n0, s))) return st;
+    if ((st = zero_launch(GFD_FLOAT32, L0.phi[0], n0, s))) return st;
+    if ((st = iterate2(ps, 0, false, s))) return st;
+    if ((st = axpby_launch(GFD_FLOAT64, ps->phi64, GFD_FLOAT32, L0.phi[0], 1.0, -1.0, n0, s)))
+      return st;
+    if ((st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1,
+                        nullptr, 0.0, ps->partials, s)))
+      return st;
+    if ((st = final_sum_launch(ps->partials,
+                               (int)op_partials(L0.op, GFD_FLOAT64, OP_RESIDUAL, 1), ps->dv,
+                               &ps->dctrl->err, s)))
+      return st;
+  }
+  launch_k(check_kernel, 1, 1, 0, s, ps->dctrl, loop, in_graph);
+  return check_launch("check_kernel");
+}
+
+// Capture the solve graph: prologue, while(loop_body), epilogue.
+static int build_graph(gfd_poisson* ps) {
+  cudaStream_t cs = nullptr;
+  int st = check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
   if (st) return st;
-  st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-  if (st) return st;
-  *out = ps->hscal[idx];
+  Level& L0 = ps->L[0];
+  const int64_t n0 = L0.n;
+  const int blocks = grid_for(n0);
+  cudaGraph_t graph = nullptr;
+  cudaGraphConditionalHandle loop;
+  cudaGraphNode_t cond_node;
+  cudaGraph_t body = nullptr;
+  auto fail = [&](int code) {
+    cudaStreamCaptureStatus cst;
+    if (cudaStreamIsCapturing(cs, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(cs, &g);
+      if (g) cudaGraphDestroy(g);
+    }
+    cudaGetLastError();
+    cudaStreamDestroy(cs);
+    return code;
+  };
+  if ((st = check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal),
+                       "cudaStreamBeginCapture")))
+    return fail(st);
+  {
+    cudaStreamCaptureStatus cst;
+    unsigned long long id;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if ((st = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, &id, &graph, &deps, &ndeps),
+                         "cudaStreamGetCaptureInfo")))
+      return fail(st);
+    if ((st = check_cuda(cudaGraphConditionalHandleCreate(&loop, graph, 1,
+                                                          cudaGraphCondAssignDefault),
+                         "cudaGraphConditionalHandleCreate")))
+      return fail(st);
+  }
+  // Prologue: charge, background, rho - background.
+  if ((st = reduce_launch(GFD_FLOAT64, ps->rho_in, n0, false, ps->dv, ps->partials,
+                          &ps->dctrl->charge, cs)))
+    return fail(st);
+  launch_k(prep_kernel, 1, 1, 0, cs, ps->dctrl, double(n0), ps->dv, loop, 1);
+  double* rho0 = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.rho) : ps->rho64;
+  launch_k(sub_bg_kernel, blocks, 256, 0, cs, rho0, ps->rho_in, ps->dctrl, n0);
+  if ((st = check_launch("prologue"))) return fail(st);
+  if (ps->precision == GFD_POISSON_MIXED) {
+    if ((st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1, nullptr,
+                        0.0, nullptr, cs)))
+      return fail(st);
+  }
+  // The loop node.
+  {
+    cudaStreamCaptureStatus cst;
+    unsigned long long id;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t g2 = nullptr;
+    if ((st = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, &id, &g2, &deps, &ndeps),
+                         "cudaStreamGetCaptureInfo")))
+      return fail(st);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = loop;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    if ((st = check_cuda(cudaGraphAddNode(&cond_node, g2, deps, ndeps, &np), "cudaGraphAddNode")))
+      return fail(st);
+    body = np.conditional.phGraph_out[0];
+    if ((st = check_cuda(cudaStreamUpdateCaptureDependencies(cs, &cond_node, 1,
+                                                             cudaStreamSetCaptureDependencies),
+                         "cudaStreamUpdateCaptureDependencies")))
+      return fail(st);
+  }
+  // Epilogue: zero mean potential for fully periodic systems.
+  double* phi_final = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.phi[0])
+                                                        : ps->phi64;
+  if (ps->pbc_all) {
+    if ((st = reduce_launch(GFD_FLOAT64, phi_final, n0, false, 1.0, ps->partials, &ps->dctrl->sum,
+                            cs)))
+      return fail(st);
+    launch_k(sub_mean_kernel, blocks, 256, 0, cs, phi_final, ps->dctrl, n0);
+    if ((st = check_launch("sub_mean_kernel"))) return fail(st);
+  }
+  if ((st = check_cuda(cudaStreamEndCapture(cs, &graph), "cudaStreamEndCapture"))) return fail(st);
+  // Populate the loop body.
+  if ((st = check_cuda(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                                     cudaStreamCaptureModeThreadLocal),
+                       "cudaStreamBeginCaptureToGraph"))) {
+    cudaGraphDestroy(graph);
+    return fail(st);
+  }
+  st = loop_body(ps, loop, 1, cs);
+  {
+    cudaGraph_t b2 = nullptr;
+    int st2 = check_cuda(cudaStreamEndCapture(cs, &b2), "cudaStreamEndCapture(body)");
+    if (!st) st = st2;
+  }
+  if (!st) {
+    cudaGraphExec_t exec = nullptr;
+    st = check_cuda(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
+    if (!st) {
+      ps->graph = graph;
+      ps->exec = exec;
+    }
+  }
+  if (st) cudaGraphDestroy(graph);
+  cudaStreamDestroy(cs);
+  return st;
+}
+
+// The solve without a graph: prologue, host-driven loop, epilogue.
+static int solve_eager(gfd_poisson* ps, cudaStream_t s) {
+  Level& L0 = ps->L[0];
+  const int64_t n0 = L0.n;
+  const int blocks = grid_for(n0);
+  int st;
+  if ((st = reduce_launch(GFD_FLOAT64, ps->rho_in, n0, false, ps->dv, ps->partials,
+                          &ps->dctrl->charge, s)))
+    return st;
+  launch_k(prep_kernel, 1, 1, 0, s, ps->dctrl, double(n0), ps->dv, cudaGraphConditionalHandle(0), 0);
+  double* rho0 = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.rho) : ps->rho64;
+  launch_k(sub_bg_kernel, blocks, 256, 0, s, rho0, ps->rho_in, ps->dctrl, n0);
+  if ((st = check_launch("prologue"))) return st;
+  if (ps->precision == GFD_POISSON_MIXED &&
+      (st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1, nullptr,
+                      0.0, nullptr, s)))
+    return st;
+  SolveCtrl* h = ps->hctrl;
+  if ((st = check_cuda(cudaMemcpyAsync(h, ps->dctrl, sizeof(SolveCtrl), cudaMemcpyDeviceToHost, s),
+                       "cudaMemcpyAsync(controls)")) ||
+      (st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+    return st;
+  if (h->status == GFD_OK) {
+    while (true) {
+      if ((st = loop_body(ps, cudaGraphConditionalHandle(0), 0, s))) return st;
+      if ((st = check_cuda(cudaMemcpyAsync(h, ps->dctrl, sizeof(SolveCtrl),
+                                           cudaMemcpyDeviceToHost, s),
+                           "cudaMemcpyAsync(controls)")) ||
+          (st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")))
+        return st;
+      if (!(h->err > h->eps && h->niter < h->maxiter)) break;
+    }
+  }
+  double* phi_final = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.phi[0])
+                                                        : ps->phi64;
+  if (ps->pbc_all) {
+    if ((st = reduce_launch(GFD_FLOAT64, phi_final, n0, false, 1.0, ps->partials, &ps->dctrl->sum,
+                            s)))
+      return st;
+    launch_k(sub_mean_kernel, blocks, 256, 0, s, phi_final, ps->dctrl, n0);
+    if ((st = check_launch("sub_mean_kernel"))) return st;
+  }
   return GFD_OK;
 }
 
@@ -137,6 +397,10 @@ extern "C" int gfd_poisson_create(int levels, gfd_operator* const* ops,
       return set_error(GFD_EINVAL, "level operator needs the diagonal as coefs[0]");
     if (relax_method == GFD_RELAX_GS && op_gs_colors(ops[l]) == 0)
       return set_error(GFD_EUNSUPPORTED, "no valid Gauss-Seidel colouring for a level operator");
+    if (presmooths[l] < 0 || postsmooths[l] < 0)
+      return set_error(GFD_EINVAL, "negative smoothing count");
+    if (relax_method != GFD_RELAX_GS && weights[l] == 0.0)
+      return set_error(GFD_EINVAL, "Jacobi weight must be nonzero");
     if (l < levels) {
       const gfd_transformer* r = restrictors[l];
       const gfd_transformer* ip = interpolators[l];
@@ -162,7 +426,6 @@ extern "C" int gfd_poisson_create(int levels, gfd_operator* const* ops,
     ps->interp.push_back(interpolators[l]);
   }
   const size_t esz = dtype_size(ps->vdtype);
-  // Layout of one pool allocation, 256-byte aligned pieces.
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t o = off;
@@ -177,55 +440,60 @@ extern "C" int gfd_poisson_create(int levels, gfd_operator* const* ops,
     lv.pre = presmooths[l];
     lv.post = postsmooths[l];
     lv.w = weights[l];
-    const bool own_phi0 = (l > 0) || (precision == GFD_POISSON_MIXED);
-    o_phi0[l] = own_phi0 ? take(lv.n * esz) : 0;
+    o_phi0[l] = take(lv.n * esz);
     o_phi1[l] = take(lv.n * esz);
     o_rho[l] = take(lv.n * esz);
     o_res[l] = take(lv.n * esz);
   }
   const int64_t n0 = ps->L[0].n;
-  size_t o_r64 = 0, o_alt64 = 0;
+  const size_t o_rho_in = take(n0 * 8);
+  size_t o_phi64 = 0, o_rho64 = 0, o_r64 = 0;
   if (precision == GFD_POISSON_MIXED) {
+    o_phi64 = take(n0 * 8);
+    o_rho64 = take(n0 * 8);
     o_r64 = take(n0 * 8);
-    o_alt64 = take(n0 * 8);
   }
-  ps->npartials = std::max<int64_t>(op_partials(ops[0], GFD_FLOAT64, OP_RESIDUAL, 1), 1);
-  size_t o_part = take(sizeof(double) * std::max<int64_t>(ps->npartials, (int64_t)kRedBlocks));
-  size_t o_scal = take(sizeof(double) * 8);
+  ps->npartials = std::max<int64_t>(op_partials(ops[0], GFD_FLOAT64, OP_RESIDUAL, 1), kRedBlocks);
+  const size_t o_part = take(sizeof(double) * ps->npartials);
+  const size_t o_ctrl = take(sizeof(SolveCtrl));
   if (cudaMalloc(&ps->pool, off) != cudaSuccess) {
     cudaGetLastError();
     delete ps;
     return set_error(GFD_ENOMEM, "cudaMalloc of the level hierarchy failed");
   }
-  if (cudaMallocHost(reinterpret_cast<void**>(&ps->hscal), sizeof(double) * 8) != cudaSuccess) {
+  if (cudaMallocHost(reinterpret_cast<void**>(&ps->hctrl), sizeof(SolveCtrl)) != cudaSuccess) {
     cudaGetLastError();
     cudaFree(ps->pool);
     delete ps;
     return set_error(GFD_ENOMEM, "cudaMallocHost failed");
   }
+  cudaGetDevice(&ps->device);
   char* base = static_cast<char*>(ps->pool);
   for (int l = 0; l <= levels; l++) {
     Level& lv = ps->L[l];
-    const bool own_phi0 = (l > 0) || (precision == GFD_POISSON_MIXED);
-    lv.phi[0] = own_phi0 ? base + o_phi0[l] : nullptr;
+    lv.phi[0] = base + o_phi0[l];
     lv.phi[1] = base + o_phi1[l];
     lv.rho = base + o_rho[l];
     lv.res = base + o_res[l];
   }
+  ps->rho_in = reinterpret_cast<double*>(base + o_rho_in);
   if (precision == GFD_POISSON_MIXED) {
-    ps->r64 = base + o_r64;
-    ps->phi64_alt = base + o_alt64;
+    ps->phi64 = reinterpret_cast<double*>(base + o_phi64);
+    ps->rho64 = reinterpret_cast<double*>(base + o_rho64);
+    ps->r64 = reinterpret_cast<double*>(base + o_r64);
   }
   ps->partials = reinterpret_cast<double*>(base + o_part);
-  ps->dscal = reinterpret_cast<double*>(base + o_scal);
+  ps->dctrl = reinterpret_cast<SolveCtrl*>(base + o_ctrl);
   *out = ps;
   return GFD_OK;
 }
 
 extern "C" int gfd_poisson_destroy(gfd_poisson* ps) {
   if (!ps) return GFD_OK;
+  if (ps->exec) cudaGraphExecDestroy(ps->exec);
+  if (ps->graph) cudaGraphDestroy(ps->graph);
   if (ps->pool) cudaFree(ps->pool);
-  if (ps->hscal) cudaFreeHost(ps->hscal);
+  if (ps->hctrl) cudaFreeHost(ps->hctrl);
   delete ps;
   return GFD_OK;
 }
@@ -237,73 +505,51 @@ extern "C" int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho
   if (!phi || !rho) return set_error(GFD_EINVAL, "null array pointer");
   if (maxiter < 1) return set_error(GFD_EINVAL, "maxiter must be >= 1");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  Level& L0 = ps->L[0];
-  const int64_t n0 = L0.n;
   int st;
-  // Charge and background (gpaw/poisson.py:130-138).
-  double actual = 0.0;
-  if ((st = reduce_launch(GFD_FLOAT64, rho, n0, false, ps->dv, ps->partials, ps->dscal + 1, s)))
+  // GFD_POISSON_EAGER=1: the same kernels launched one by one with a host
+  // loop (one wait per V-cycle), for per-kernel profiling.
+  static const bool eager = [] {
+    const char* e = getenv("GFD_POISSON_EAGER");
+    return e && e[0] == '1';
+  }();
+  if (!eager && !ps->exec && (st = build_graph(ps))) return st;
+  const int64_t n0 = ps->L[0].n;
+  double* phi_int = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
+                                                      : ps->phi64;
+  SolveCtrl* h = ps->hctrl;
+  h->eps = eps;
+  h->maxcharge = maxcharge;
+  h->charge_arg = charge;
+  h->maxiter = maxiter;
+  if ((st = check_cuda(cudaMemcpyAsync(ps->dctrl, h, offsetof(SolveCtrl, charge),
+                                       cudaMemcpyHostToDevice, s),
+                       "cudaMemcpyAsync(controls)")))
     return st;
-  if ((st = read_scalar(ps, 1, &actual, s))) return st;
-  const double background = actual / ps->dv / double(n0);
-  const double q = std::isnan(charge) ? actual : charge;
-  if (std::fabs(q) > maxcharge)
+  if ((st = check_cuda(cudaMemcpyAsync(ps->rho_in, rho, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                       "cudaMemcpyAsync(rho)")))
+    return st;
+  if ((st = check_cuda(cudaMemcpyAsync(phi_int, phi, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                       "cudaMemcpyAsync(phi)")))
+    return st;
+  if (!eager) {
+    if ((st = check_cuda(cudaGraphLaunch(ps->exec, s), "cudaGraphLaunch"))) return st;
+  } else if ((st = solve_eager(ps, s))) {
+    return st;
+  }
+  if ((st = check_cuda(cudaMemcpyAsync(h, ps->dctrl, sizeof(SolveCtrl), cudaMemcpyDeviceToHost, s),
+                       "cudaMemcpyAsync(controls)")))
+    return st;
+  if ((st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize(solve)"))) return st;
+  if (h->status == GFD_EUNSUPPORTED)
     return set_error(GFD_EUNSUPPORTED,
                      "charged system: only the charge-neutral branch of solve() is provided");
-
-  int niter = 1;
-  double err = 0.0;
-  if (ps->precision == GFD_POISSON_FP64) {
-    // rhos[0] = rho - background; phis[0] = phi
-    L0.phi[0] = phi;
-    L0.cur = 0;
-    if ((st = sub_const_launch(GFD_FLOAT64, L0.rho, rho, background, n0, s))) return st;
-    while (true) {
-      if ((st = iterate2(ps, 0, true, s))) return st;
-      if ((st = read_scalar(ps, 0, &err, s))) return st;
-      if (!(err > eps) || niter >= maxiter) break;
-      niter++;
-    }
-    if (L0.cur != 0 &&
-        (st = check_cuda(cudaMemcpyAsync(phi, L0.phi[L0.cur], n0 * 8, cudaMemcpyDeviceToDevice, s),
-                         "cudaMemcpyAsync(phi)")))
-      return st;
-  } else {
-    // Mixed: float64 rho0 in r64's sibling; residual r = L phi - rho0.
-    double* rho0 = static_cast<double*>(ps->phi64_alt);
-    double* r64 = static_cast<double*>(ps->r64);
-    if ((st = sub_const_launch(GFD_FLOAT64, rho0, rho, background, n0, s))) return st;
-    if ((st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, phi, r64, rho0, 1, nullptr, 0.0, nullptr,
-                        s)))
-      return st;
-    while (true) {
-      if ((st = convert_launch(GFD_FLOAT32, L0.rho, GFD_FLOAT64, r64, n0, s))) return st;
-      L0.cur = 0;
-      if ((st = check_cuda(cudaMemsetAsync(L0.phi[0], 0, n0 * 4, s), "cudaMemsetAsync"))) return st;
-      if ((st = iterate2(ps, 0, false, s))) return st;
-      if ((st = axpby_launch(GFD_FLOAT64, phi, GFD_FLOAT32, L0.phi[L0.cur], 1.0, -1.0, n0, s)))
-        return st;
-      if ((st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, phi, r64, rho0, 1, nullptr, 0.0,
-                          ps->partials, s)))
-        return st;
-      if ((st = final_sum_launch(ps->partials, (int)ps->npartials, ps->dv, ps->dscal, s))) return st;
-      if ((st = read_scalar(ps, 0, &err, s))) return st;
-      if (!(err > eps) || niter >= maxiter) break;
-      niter++;
-    }
-  }
-  if (niter_out) *niter_out = niter;
-  if (error_out) *error_out = err;
-  if (niter == maxiter)
+  if (niter_out) *niter_out = h->niter;
+  if (error_out) *error_out = h->err;
+  if ((st = check_cuda(cudaMemcpyAsync(phi, phi_int, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                       "cudaMemcpyAsync(phi)")))
+    return st;
+  if (h->niter >= maxiter)
     return set_error(GFD_ENOCONV, "Poisson solver did not converge in " +
                                       std::to_string(maxiter) + " iterations!");
-  // Zero mean potential for fully periodic systems (gpaw/poisson.py:212-216).
-  if (ps->pbc_all) {
-    double sum = 0.0;
-    if ((st = reduce_launch(GFD_FLOAT64, phi, n0, false, 1.0, ps->partials, ps->dscal + 1, s)))
-      return st;
-    if ((st = read_scalar(ps, 1, &sum, s))) return st;
-    if ((st = sub_const_launch(GFD_FLOAT64, phi, phi, sum / double(n0), n0, s))) return st;
-  }
-  return check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize(solve)");
+  return GFD_OK;
 }

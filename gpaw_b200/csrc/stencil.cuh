@@ -119,6 +119,7 @@ template <class V, int R, int BZ, int TY, int VY, int S, int MODE>
 __global__ void __launch_bounds__(BZ * TY)
 star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
             const StarParams<typename vt<V>::S> p) {
+  pdl_enter();
   using Sc = typename vt<V>::S;
   constexpr int NT = BZ * TY, BY = TY * VY;
   constexpr int SY = BY + 2 * R, SZ = BZ + 2 * R, CELLS = SY * SZ;
@@ -361,6 +362,73 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
 }
 
 // ---------------------------------------------------------------------------
+// Direct star stencil: one thread per point, neighbours read through the L1
+// cache.  For small grids (the coarse multigrid levels) the marching kernel
+// is latency-bound -- each plane step waits for a memory round trip -- while
+// this kernel finishes in about one round trip.  Same modes and arithmetic
+// as star_kernel (folded Jacobi centre weight included).  Grid-stride over
+// nin * n0 * n1 * n2 points with a fixed grid, so the per-CTA partial sums
+// of MODE_RESIDUAL have a fixed order.
+// ---------------------------------------------------------------------------
+template <class V, int R, int MODE>
+__global__ void __launch_bounds__(256)
+star_direct_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
+                   const StarParams<typename vt<V>::S> p, long long total) {
+  pdl_enter();
+  __shared__ double red[8];
+  const long long plane = (long long)p.n1 * p.n2;
+  double sumsq = 0.0;
+  for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256) {
+    const long long b = g / p.band;
+    const long long rem = g - b * p.band;
+    const int i0 = int(rem / plane);
+    const int r1 = int(rem - i0 * plane);
+    const int i1 = r1 / p.n2, i2 = r1 - i1 * p.n2;
+    const V* base = in + b * p.band;
+    V s = vmul(p.c0, ldro(in + g));
+#pragma unroll
+    for (int k = -R; k <= R; k++) {
+      if (k == 0) continue;
+      int sd;
+      int j = wrap_axis(i0 + k, p.n0, p.per0, sd);
+      if (j >= 0) {
+        V v = ldro(base + j * plane + r1);
+        if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 0, sd), v); }
+        madd(s, p.cx[kMaxR + k], v);
+      }
+      j = wrap_axis(i1 + k, p.n1, p.per1, sd);
+      if (j >= 0) {
+        V v = ldro(base + i0 * plane + j * p.n2 + i2);
+        if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 1, sd), v); }
+        madd(s, p.cy[kMaxR + k], v);
+      }
+      j = wrap_axis(i2 + k, p.n2, p.per2, sd);
+      if (j >= 0) {
+        V v = ldro(base + i0 * plane + i1 * p.n2 + j);
+        if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 2, sd), v); }
+        madd(s, p.cz[kMaxR + k], v);
+      }
+    }
+    if constexpr (MODE == MODE_APPLY) {
+      out[g] = s;
+    } else if constexpr (MODE == MODE_JACOBI) {
+      static_assert(vt<V>::NC == 1, "relaxation is real only");
+      out[g] = p.wc * (ldro(rho + g) - s);
+    } else {
+      const V r = vsub(s, ldro(rho + g));
+      out[g] = r;
+      if constexpr (vt<V>::NC == 1) sumsq += sq(r);
+    }
+  }
+  if constexpr (MODE == MODE_RESIDUAL) {
+    if (p.partials) {
+      const double sblk = block_sum<256>(sumsq, red);
+      if (threadIdx.x == 0) p.partials[blockIdx.x] = sblk;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // General stencil: any offsets within +-MP on every axis.
 // ---------------------------------------------------------------------------
 template <class S>
@@ -381,6 +449,7 @@ template <class V, int BZ, int TY, int VY, int MODE>
 __global__ void __launch_bounds__(BZ * TY)
 general_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
                const GenParams<typename vt<V>::S> p, int mp) {
+  pdl_enter();
   using S = typename vt<V>::S;
   constexpr int NT = BZ * TY, BY = TY * VY;
   const int SY = BY + 2 * mp, SZ = BZ + 2 * mp, NR = 2 * mp + 1;
@@ -477,6 +546,7 @@ template <class V>
 __global__ void __launch_bounds__(256)
 color_gs_kernel(V* __restrict__ phi, const V* __restrict__ rho, const V* __restrict__ frozen,
                 const GenParams<typename vt<V>::S> p, int ncolor, int color) {
+  pdl_enter();
   using S = typename vt<V>::S;
   const long long n = (long long)p.n0 * p.n1 * p.n2;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n;

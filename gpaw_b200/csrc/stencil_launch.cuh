@@ -35,6 +35,19 @@ inline TileDims tile_dims(int tile) {
 
 constexpr int kStages = 4;
 
+// Grids up to this many points (all bands) use the one-thread-per-point
+// kernel: the marching kernel's plane pipeline only pays off on larger grids.
+constexpr long long kDirectMaxPoints = 300000;
+
+inline bool use_direct(const gfd_operator* op, int64_t nin) {
+  return (long long)op->n[0] * op->n[1] * op->n[2] * nin <= kDirectMaxPoints;
+}
+inline int direct_blocks(long long total) {
+  long long b = (total + 255) / 256;
+  long long cap = 8LL * num_sms();
+  return int(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
 // Raise a kernel's dynamic shared-memory limit when it needs more than 48 KB.
 template <class F>
 int raise_smem_limit(F* kern, size_t bytes, const char* what) {
@@ -90,7 +103,7 @@ int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t n
     int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
     dim3 grid(g.grid.x, g.grid.y, (unsigned)(nb * g.nxc));
     p.partials = partials ? partials + b0 * g.nxc * g.grid.x * g.grid.y : nullptr;
-    kern<<<grid, BZ * TY, smem, s>>>(in + b0 * band, out + b0 * band,
+    launch_k(kern, grid, BZ * TY, smem, s, in + b0 * band, out + b0 * band,
                                      rho ? rho + b0 * band : nullptr, p);
   }
   return check_launch("star_kernel");
@@ -136,6 +149,22 @@ int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V
   return set_error(GFD_EUNSUPPORTED, "star stencil radius out of range");
 }
 
+template <class V, int MODE>
+int direct_dispatch(const gfd_operator* op, const V* in, V* out, const V* rho,
+                    const StarParams<typename vt<V>::S>& p, long long total, cudaStream_t s) {
+  const int blocks = direct_blocks(total);
+  switch (op->R) {
+    case 1: launch_k(star_direct_kernel<V, 1, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+    case 2: launch_k(star_direct_kernel<V, 2, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+    case 3: launch_k(star_direct_kernel<V, 3, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+    case 4: launch_k(star_direct_kernel<V, 4, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+    case 5: launch_k(star_direct_kernel<V, 5, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+    case 6: launch_k(star_direct_kernel<V, 6, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+    default: return set_error(GFD_EUNSUPPORTED, "star stencil radius out of range");
+  }
+  return check_launch("star_direct_kernel");
+}
+
 template <class V>
 int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* out, const void* rho,
                       int64_t nin, const double* phase_cd, double w, double* partials,
@@ -163,20 +192,31 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
       for (int d = 0; d < 2; d++)
         if (op->per[c] && (phase_cd[4 * c + 2 * d] != 1.0 || phase_cd[4 * c + 2 * d + 1] != 0.0))
           p.fix_yz = 1;
+  const V* vin = static_cast<const V*>(in);
+  V* vout = static_cast<V*>(out);
+  const V* vrho = static_cast<const V*>(rho);
+  if constexpr (vt<V>::NC == 2) {
+    if (mode != OP_APPLY) return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
+  }
+  if (use_direct(op, nin)) {
+    p.partials = partials;
+    const long long total = (long long)p.band * nin;
+    if constexpr (vt<V>::NC == 1) {
+      if (mode == OP_JACOBI) return direct_dispatch<V, MODE_JACOBI>(op, vin, vout, vrho, p, total, s);
+      if (mode == OP_RESIDUAL)
+        return direct_dispatch<V, MODE_RESIDUAL>(op, vin, vout, vrho, p, total, s);
+    }
+    return direct_dispatch<V, MODE_APPLY>(op, vin, vout, nullptr, p, total, s);
+  }
   const int tile = pick_tile(op);
   LaunchGeom g = star_geom(op, tile, nin, op->R);
   p.nxc = g.nxc;
   p.x_chunk = g.x_chunk;
-  const V* vin = static_cast<const V*>(in);
-  V* vout = static_cast<V*>(out);
-  const V* vrho = static_cast<const V*>(rho);
   if constexpr (vt<V>::NC == 1) {
     if (mode == OP_JACOBI)
       return star_dispatch<V, MODE_JACOBI>(op, tile, vin, vout, vrho, nin, p, g, nullptr, s);
     if (mode == OP_RESIDUAL)
       return star_dispatch<V, MODE_RESIDUAL>(op, tile, vin, vout, vrho, nin, p, g, partials, s);
-  } else {
-    if (mode != OP_APPLY) return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
   }
   return star_dispatch<V, MODE_APPLY>(op, tile, vin, vout, nullptr, nin, p, g, nullptr, s);
 }
@@ -203,7 +243,7 @@ int general_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_
     int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
     dim3 grid(gx, gy, (unsigned)(nb * g.nxc));
     p.partials = partials ? partials + b0 * g.nxc * gx * gy : nullptr;
-    general_kernel<V, BZ, TY, VY, MODE><<<grid, BZ * TY, smem, s>>>(
+    launch_k(general_kernel<V, BZ, TY, VY, MODE>, grid, BZ * TY, smem, s, 
         in + b0 * band, out + b0 * band, rho ? rho + b0 * band : nullptr, p, mp);
   }
   return check_launch("general_kernel");
@@ -240,6 +280,8 @@ int launch_general_typed(const gfd_operator* op, int mode, const void* in, void*
 }
 
 inline int64_t partials_count(const gfd_operator* op, int64_t nin) {
+  if (op->star && use_direct(op, nin))
+    return direct_blocks((long long)op->n[0] * op->n[1] * op->n[2] * nin);
   if (op->star) {
     int tile = pick_tile(op);
     TileDims td = tile_dims(tile);
@@ -275,7 +317,7 @@ int gs_typed(const gfd_operator* op, V* phi, const V* rho, int nsweeps, V* froze
       if (e != cudaSuccess) return check_cuda(e, "cudaMemcpyAsync(frozen)");
     }
     for (int c = 0; c < ncolor; c++)
-      color_gs_kernel<V><<<blocks, 256, 0, s>>>(phi, rho, any_per ? frozen : phi, p, ncolor, c);
+      launch_k(color_gs_kernel<V>, blocks, 256, 0, s, phi, rho, any_per ? frozen : phi, p, ncolor, c);
   }
   return check_launch("color_gs_kernel");
 }

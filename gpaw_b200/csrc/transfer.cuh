@@ -93,6 +93,7 @@ template <class V, int NN, int BZC, int TYC, int VYC>
 __global__ void __launch_bounds__(BZC * TYC)
 restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
                 const TrParams<typename vt<V>::S> p) {
+  pdl_enter();
   using S = typename vt<V>::S;
   constexpr int NT = BZC * TYC, BYC = TYC * VYC;
   constexpr int W = 2 * NN - 1;           // wing of one restriction tap
@@ -203,10 +204,13 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
 // (nn-1) + i and (nn-1) + i + 1 (c/bmgs/interpolate.c:19-66).  Coarse array
 // index of step i: c(i) = i + nn - 1 - lo.
 // ---------------------------------------------------------------------------
-template <class V, int NN, int BZF, int TYF, int VYF>
+// SUB: out = base - interpolated value (the multigrid correction
+// phi -= interpolate(e), in place when base == out).
+template <class V, int NN, int BZF, int TYF, int VYF, bool SUB>
 __global__ void __launch_bounds__(BZF * TYF)
-interp_kernel(const V* __restrict__ in, V* __restrict__ out,
+interp_kernel(const V* __restrict__ in, V* out, const V* base,
               const TrParams<typename vt<V>::S> p) {
+  pdl_enter();
   using S = typename vt<V>::S;
   constexpr int NT = BZF * TYF, BYF = TYF * VYF;
   constexpr int CY = BYF / 2 + 2 * NN, CZ = BZF / 2 + 2 * NN;
@@ -225,6 +229,7 @@ interp_kernel(const V* __restrict__ in, V* __restrict__ out,
   const long long plane_out = (long long)p.no1 * p.no2;
   const V* inb = in + bnd * p.band_in;
   V* outb = out + bnd * p.band_out;
+  const V* baseb = SUB ? base + bnd * p.band_out : nullptr;
   const int iy0 = (Y0 + p.sk1) >> 1, iz0 = (Z0 + p.sk2) >> 1;
   const int cy0 = iy0 - p.lo1, cz0 = iz0 - p.lo2;  // coarse origin of the tile
 
@@ -308,11 +313,88 @@ interp_kernel(const V* __restrict__ in, V* __restrict__ out,
           const int y = Y0 + ty + j * TYF, z = Z0 + tz;
           if (y < p.no1 && z < p.no2) {
             V v = par ? ip_tap<NN, V>([&](int o) { return q[j][NN - 1 + o]; }) : q[j][NN - 1];
-            stcs(outb + X * plane_out + (long long)y * p.no2 + z, v);
+            const long long o = X * plane_out + (long long)y * p.no2 + z;
+            if constexpr (SUB) v = vsub(baseb[o], v);
+            stcs(outb + o, v);
           }
         }
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Direct forms for small grids (coarse multigrid levels): one thread per
+// output point, the three 1-D passes nested in registers in the reference's
+// order (axis 2 innermost, then axis 1, then axis 0), neighbours read through
+// the L1 cache.  The marching kernels above pay a memory round trip per plane,
+// which dominates on grids of a few thousand points.
+// ---------------------------------------------------------------------------
+template <class V, class S>
+__device__ __forceinline__ V tr_fetch(const V* base, int x, int y, int z, const TrParams<S>& p) {
+  int sx, sy, sz;
+  const int i = wrap_axis(x, p.ni0, p.per0, sx);
+  const int j = wrap_axis(y, p.ni1, p.per1, sy);
+  const int k = wrap_axis(z, p.ni2, p.per2, sz);
+  if (i < 0 || j < 0 || k < 0) return vzero<V>();
+  V v = ldro(base + ((long long)i * p.ni1 + j) * p.ni2 + k);
+  if constexpr (vt<V>::NC == 2) {
+    if (sx >= 0) v = phase_mul(phase_of(p.P, 0, sx), v);
+    if (sy >= 0) v = phase_mul(phase_of(p.P, 1, sy), v);
+    if (sz >= 0) v = phase_mul(phase_of(p.P, 2, sz), v);
+  }
+  return v;
+}
+
+template <class V, int NN>
+__global__ void __launch_bounds__(256)
+restrict_direct_kernel(const V* __restrict__ in, V* __restrict__ out,
+                       const TrParams<typename vt<V>::S> p, long long total) {
+  pdl_enter();
+  constexpr int W = 2 * NN - 1;
+  const long long plane_out = (long long)p.no1 * p.no2;
+  for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256) {
+    const long long b = g / p.band_out;
+    const long long rem = g - b * p.band_out;
+    const int X = int(rem / plane_out);
+    const int r1 = int(rem - X * plane_out);
+    const int Y = r1 / p.no2, Z = r1 - Y * p.no2;
+    const V* base = in + b * p.band_in;
+    // fine centre of each axis: 2i + (2nn-1) - lo
+    const int fx = 2 * X + W - p.lo0, fy = 2 * Y + W - p.lo1, fz = 2 * Z + W - p.lo2;
+    out[g] = rst_tap<NN, V>([&](int ox) {
+      return rst_tap<NN, V>([&](int oy) {
+        return rst_tap<NN, V>([&](int oz) { return tr_fetch(base, fx + ox, fy + oy, fz + oz, p); });
+      });
+    });
+  }
+}
+
+template <class V, int NN, bool SUB>
+__global__ void __launch_bounds__(256)
+interp_direct_kernel(const V* __restrict__ in, V* out, const V* base_out,
+                     const TrParams<typename vt<V>::S> p, long long total) {
+  pdl_enter();
+  const long long plane_out = (long long)p.no1 * p.no2;
+  for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256) {
+    const long long b = g / p.band_out;
+    const long long rem = g - b * p.band_out;
+    const int X = int(rem / plane_out);
+    const int r1 = int(rem - X * plane_out);
+    const int Y = r1 / p.no2, Z = r1 - Y * p.no2;
+    const V* base = in + b * p.band_in;
+    // g = f + skip[c][0]; even g: coarse point c(i) = i + nn - 1 - lo, odd: between c(i), c(i)+1
+    const int gx = X + p.sk0, gy = Y + p.sk1, gz = Z + p.sk2;
+    const int cx = (gx >> 1) + NN - 1 - p.lo0, cy = (gy >> 1) + NN - 1 - p.lo1,
+              cz = (gz >> 1) + NN - 1 - p.lo2;
+    auto along = [&](int odd, auto get) -> V { return odd ? ip_tap<NN, V>(get) : get(0); };
+    V v = along(gx & 1, [&](int ox) {
+      return along(gy & 1, [&](int oy) {
+        return along(gz & 1, [&](int oz) { return tr_fetch(base, cx + ox, cy + oy, cz + oz, p); });
+      });
+    });
+    if constexpr (SUB) v = vsub(base_out[g], v);
+    out[g] = v;
   }
 }
 

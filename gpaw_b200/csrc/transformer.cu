@@ -40,13 +40,13 @@ static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t n
   for (int64_t b0 = 0; b0 < nin; b0 += per_launch) {
     int64_t nb = std::min<int64_t>(per_launch, nin - b0);
     dim3 grid(gx, gy, (unsigned)(nb * p.nxc));
-    kern<<<grid, BZC * TYC, smem, s>>>(in + b0 * p.band_in, out + b0 * p.band_out, p);
+    launch_k(kern, grid, BZC * TYC, smem, s, in + b0 * p.band_in, out + b0 * p.band_out, p);
   }
   return check_launch("restrict_kernel");
 }
 
 template <class V, int NN>
-static int interp_go(const gfd_transformer* tr, const V* in, V* out, int64_t nin,
+static int interp_go(const gfd_transformer* tr, const V* in, V* out, const V* base, int64_t nin,
                      TrParams<typename vt<V>::S>& p, cudaStream_t s) {
   constexpr int BZF = 64, TYF = 4, VYF = 2, BYF = TYF * VYF;
   constexpr int CY = BYF / 2 + 2 * NN, CZ = BZF / 2 + 2 * NN;
@@ -58,21 +58,41 @@ static int interp_go(const gfd_transformer* tr, const V* in, V* out, int64_t nin
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   p.x_chunk = (tr->nout[0] + nxc - 1) / nxc;
   p.nxc = (tr->nout[0] + p.x_chunk - 1) / p.x_chunk;
-  auto kern = interp_kernel<V, NN, BZF, TYF, VYF>;
+  auto kern = base ? interp_kernel<V, NN, BZF, TYF, VYF, true>
+                   : interp_kernel<V, NN, BZF, TYF, VYF, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute(interp_kernel)");
   const int64_t per_launch = std::max<int64_t>(1, 65535 / p.nxc);
   for (int64_t b0 = 0; b0 < nin; b0 += per_launch) {
     int64_t nb = std::min<int64_t>(per_launch, nin - b0);
     dim3 grid(gx, gy, (unsigned)(nb * p.nxc));
-    kern<<<grid, BZF * TYF, smem, s>>>(in + b0 * p.band_in, out + b0 * p.band_out, p);
+    launch_k(kern, grid, BZF * TYF, smem, s, in + b0 * p.band_in, out + b0 * p.band_out,
+                                       base ? base + b0 * p.band_out : nullptr, p);
   }
   return check_launch("interp_kernel");
 }
 
+// Outputs (all bands) up to this count use the one-thread-per-point forms.
+constexpr long long kTrDirectMaxPoints = 300000;
+
+template <class V, int NN>
+static int direct_go(const gfd_transformer* tr, const V* in, V* out, const V* base, int64_t nin,
+                     const TrParams<typename vt<V>::S>& p, cudaStream_t s) {
+  const long long total = p.band_out * nin;
+  long long b = (total + 255) / 256, cap = 8LL * num_sms();
+  const int blocks = int(b < 1 ? 1 : (b > cap ? cap : b));
+  if (!tr->interpolate)
+    launch_k(restrict_direct_kernel<V, NN>, blocks, 256, 0, s, in, out, p, total);
+  else if (base)
+    launch_k(interp_direct_kernel<V, NN, true>, blocks, 256, 0, s, in, out, base, p, total);
+  else
+    launch_k(interp_direct_kernel<V, NN, false>, blocks, 256, 0, s, in, out, nullptr, p, total);
+  return check_launch("transfer_direct_kernel");
+}
+
 template <class V>
-static int tr_typed(const gfd_transformer* tr, const void* in, void* out, int64_t nin,
-                    const double* ph, cudaStream_t s) {
+static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const void* base_v,
+                    int64_t nin, const double* ph, cudaStream_t s) {
   using S = typename vt<V>::S;
   TrParams<S> p{};
   p.ni0 = tr->nin[0]; p.ni1 = tr->nin[1]; p.ni2 = tr->nin[2];
@@ -85,14 +105,26 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, int64_
   fill_tr_phases(p.P, ph);
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
+  const V* base = static_cast<const V*>(base_v);
+  if (base && !tr->interpolate)
+    return set_error(GFD_EINVAL, "subtracting form is for interpolation only");
+  if (p.band_out * nin <= kTrDirectMaxPoints) {
+    switch (tr->nn) {
+      case 1: return direct_go<V, 1>(tr, vin, vout, base, nin, p, s);
+      case 2: return direct_go<V, 2>(tr, vin, vout, base, nin, p, s);
+      case 3: return direct_go<V, 3>(tr, vin, vout, base, nin, p, s);
+      case 4: return direct_go<V, 4>(tr, vin, vout, base, nin, p, s);
+    }
+  }
   if (tr->interpolate) {
     switch (tr->nn) {
-      case 1: return interp_go<V, 1>(tr, vin, vout, nin, p, s);
-      case 2: return interp_go<V, 2>(tr, vin, vout, nin, p, s);
-      case 3: return interp_go<V, 3>(tr, vin, vout, nin, p, s);
-      case 4: return interp_go<V, 4>(tr, vin, vout, nin, p, s);
+      case 1: return interp_go<V, 1>(tr, vin, vout, base, nin, p, s);
+      case 2: return interp_go<V, 2>(tr, vin, vout, base, nin, p, s);
+      case 3: return interp_go<V, 3>(tr, vin, vout, base, nin, p, s);
+      case 4: return interp_go<V, 4>(tr, vin, vout, base, nin, p, s);
     }
   } else {
+    if (base) return set_error(GFD_EINVAL, "subtracting form is for interpolation only");
     switch (tr->nn) {
       case 1: return restrict_go<V, 1>(tr, vin, vout, nin, p, s);
       case 2: return restrict_go<V, 2>(tr, vin, vout, nin, p, s);
@@ -103,16 +135,21 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, int64_
   return set_error(GFD_EINVAL, "k must be 2, 4, 6 or 8");
 }
 
-int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,
-              const double* phases, cudaStream_t s) {
+int tr_launch_sub(const gfd_transformer* tr, int dtype, const void* in, void* out,
+                  const void* base, int64_t nin, const double* phases, cudaStream_t s) {
   if (nin <= 0) return GFD_OK;
   switch (dtype) {
-    case GFD_FLOAT64: return tr_typed<double>(tr, in, out, nin, phases, s);
-    case GFD_FLOAT32: return tr_typed<float>(tr, in, out, nin, phases, s);
-    case GFD_COMPLEX128: return tr_typed<cplx<double>>(tr, in, out, nin, phases, s);
-    case GFD_COMPLEX64: return tr_typed<cplx<float>>(tr, in, out, nin, phases, s);
+    case GFD_FLOAT64: return tr_typed<double>(tr, in, out, base, nin, phases, s);
+    case GFD_FLOAT32: return tr_typed<float>(tr, in, out, base, nin, phases, s);
+    case GFD_COMPLEX128: return tr_typed<cplx<double>>(tr, in, out, base, nin, phases, s);
+    case GFD_COMPLEX64: return tr_typed<cplx<float>>(tr, in, out, base, nin, phases, s);
   }
   return set_error(GFD_EINVAL, "unknown dtype");
+}
+
+int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,
+              const double* phases, cudaStream_t s) {
+  return tr_launch_sub(tr, dtype, in, out, nullptr, nin, phases, s);
 }
 
 }  // namespace gfd

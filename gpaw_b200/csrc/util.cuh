@@ -15,6 +15,7 @@ constexpr int kRedThreads = 256;
 template <class Y, class X>
 __global__ void __launch_bounds__(256) axpby_kernel(Y* __restrict__ y, const X* __restrict__ x,
                                                     double a, double b, long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = Y(a * double(y[i]) + b * double(x[i]));
@@ -23,16 +24,28 @@ __global__ void __launch_bounds__(256) axpby_kernel(Y* __restrict__ y, const X* 
 // y[i] = x[i] - c  (background removal; y may alias x)
 template <class T>
 __global__ void __launch_bounds__(256) sub_const_kernel(T* y, const T* x, double c, long long n) {
+  pdl_enter();
   const T cc = T(c);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = x[i] - cc;
 }
 
+// y[i] = 0 (a kernel rather than a memset node, so the chain of kernels in
+// a captured graph stays programmatic)
+template <class T>
+__global__ void __launch_bounds__(256) zero_kernel(T* __restrict__ y, long long n) {
+  pdl_enter();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = T(0);
+}
+
 // y[i] = T(x[i])
 template <class Y, class X>
 __global__ void __launch_bounds__(256) convert_kernel(Y* __restrict__ y, const X* __restrict__ x,
                                                       long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = Y(x[i]);
@@ -43,6 +56,7 @@ template <class T, bool SQUARE>
 __global__ void __launch_bounds__(kRedThreads) partial_sum_kernel(const T* __restrict__ a,
                                                                   long long n,
                                                                   double* __restrict__ partials) {
+  pdl_enter();
   __shared__ double red[kRedThreads / 32];
   double s = 0.0;
   for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n;
@@ -64,6 +78,7 @@ __global__ void __launch_bounds__(kRedThreads) partial_sum_kernel(const T* __res
 static __global__ void __launch_bounds__(kRedThreads) final_sum_kernel(const double* __restrict__ partials,
                                                                 int n, double scale,
                                                                 double* __restrict__ out) {
+  pdl_enter();
   __shared__ double red[kRedThreads];
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += kRedThreads) s += partials[i];
