@@ -298,6 +298,104 @@ def poisson_bench(nsolves=8):
 
 
 # ---------------------------------------------------------------------------
+# Poisson serving: requests arriving as a Poisson process, grids drawn from
+# {32, 48, 64, 96, 128, 160}^3 (zero boundary, h = 0.2 A), rho a pair density
+# of two 8-Gaussian orbitals, eps = 2e-10, 120 GB admission budget.
+# ---------------------------------------------------------------------------
+SERVING_SIZES = (32, 48, 64, 96, 128, 160)
+
+
+def serving_bench(rates=(1000.0, 5000.0), nreq=300, precisions=('fp64', 'mixed'), seed=5):
+    import torch
+    from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
+    h = 0.2 / BOHR
+    rng = np.random.default_rng(seed)
+    # Four pre-generated densities per grid size; request i uses one of them
+    # (the solve work depends on the grid, not on which density).
+    dens = {N: [pair_density(grid_for(N, h), 1000 * N + k) for k in range(4)]
+            for N in SERVING_SIZES}
+    torch.cuda.synchronize()
+    out = {'workload': '%d requests per rate, grids %s^3 zero boundary, h=0.2 A, pair densities, '
+                       'eps=2e-10, budget 120 GB' % (nreq, list(SERVING_SIZES))}
+    for prec in precisions:
+        srv = PoissonServer(h, precision=prec, max_inflight=64, nstreams=32)
+        srv.warm(SERVING_SIZES, per_size=24)
+        res = {}
+        for lam in rates:
+            gaps = rng.exponential(1.0 / lam, nreq)
+            t = np.cumsum(gaps) - gaps[0]
+            sizes = rng.choice(SERVING_SIZES, nreq)
+            reqs = [Request(i, int(N), float(t[i]), dens[int(N)][i % 4]) for i, N in enumerate(sizes)]
+            srv.run(reqs[:16])  # warm the pools for this rate (not timed)
+            stats = srv.run(reqs)
+            res['%g/s' % lam] = {k: stats[k] for k in ('completed', 'solves_per_s', 'p50_ms',
+                                                         'p99_ms', 'max_err', 'rejected')}
+        res['device_bytes'] = srv.used_bytes
+        out[prec] = res
+    return out
+
+
+def batch_bench():
+    """32 simultaneous solves (8 each of 48, 64, 80, 96 points per axis, 16
+    Gaussians, multicolour Gauss-Seidel) in one graph launch, and band-
+    batched restriction/interpolation of 256 float64 bands 224^3 <-> 112^3
+    (nn=3, periodic)."""
+    import torch
+    from gpaw_b200.poisson import PoissonSolver
+    from gpaw_b200.serving import PoissonBatch, grid_for
+    from gpaw_b200.transformers import Transformer
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    h = 0.2 / BOHR
+    solvers, rhos, phis = [], [], []
+    for i, N in enumerate([48] * 8 + [64] * 8 + [80] * 8 + [96] * 8):
+        gd = grid_for(N, h)
+        ps = PoissonSolver(3, 'GS', 2e-10)
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        solvers.append(ps)
+        rhos.append(torch.from_numpy(poisson_rho(gd, 16, 40 + i)).cuda())
+        phis.append(torch.zeros_like(rhos[-1]))
+    batch = PoissonBatch(solvers)
+    batch.solve(phis, rhos)  # warm-up (captures the graph)
+    for p in phis:
+        p.zero_()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = batch.solve(phis, rhos)
+    dt = time.perf_counter() - t0
+    out = {'poisson_batch': {'workload': '32 solves, 8 each of 48,64,80,96^3, GS, one launch',
+                             'seconds': dt, 'solves_per_s': 32 / dt,
+                             'vcycles': [r[0] for r in res], 'max_residual': max(r[1] for r in res)}}
+    coarse = GridDescriptor((112,) * 3, (112 * 0.3,) * 3, 1)
+    fine = coarse.refine()
+    g = torch.Generator(device='cuda')
+    g.manual_seed(4)
+    c = torch.rand((256, 112, 112, 112), dtype=torch.float64, device='cuda', generator=g) * 2 - 1
+    f = torch.empty((256, 224, 224, 224), dtype=torch.float64, device='cuda')
+    ip = Transformer(coarse, fine, 3)
+    rs = Transformer(fine, coarse, 3)
+    for _ in range(2):
+        ip.apply(c, f)
+        rs.apply(f, c)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    ip.apply(c, f)
+    ev[1].record()
+    rs.apply(f, c)
+    ev[2].record()
+    torch.cuda.synchronize()
+    nfine = 256 * 224 ** 3
+    t_ip = ev[0].elapsed_time(ev[1]) * 1e-3
+    t_rs = ev[1].elapsed_time(ev[2]) * 1e-3
+    out['transfers'] = {'workload': '256 float64 bands, 112^3 <-> 224^3, nn=3, periodic',
+                        'interpolate_GBps': 9 * nfine / t_ip / 1e9,
+                        'restrict_GBps': 9 * nfine / t_rs / 1e9,
+                        'interpolate_ms': t_ip * 1e3, 'restrict_ms': t_rs * 1e3}
+    del c, f
+    return out
+
+
+# ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args):
@@ -384,6 +482,12 @@ def run_gpu_arm(args):
             line['poisson'] = pb
         except Exception as e:  # reported, never hidden
             line['poisson'] = {'error': repr(e)}
+    if rank == 0 and world == 1 and not args.no_poisson and not args.no_serving:
+        try:
+            line['serving'] = serving_bench(nreq=args.requests)
+            line.update(batch_bench())
+        except Exception as e:  # reported, never hidden
+            line['serving'] = {'error': repr(e)}
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = CpuStencil(16)
         r, reps, dt = cpu.rate(args.cpu_seconds)
@@ -411,17 +515,24 @@ def main():
     ap.add_argument('--cpu-seconds', type=float, default=10.0)
     ap.add_argument('--no-poisson', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
-    ap.add_argument('--only', choices=['poisson'], default=None,
+    ap.add_argument('--only', choices=['poisson', 'serving', 'batch'], default=None,
                     help='run only the Poisson solves/s sub-benchmark (profiling)')
     ap.add_argument('--solves', type=int, default=8, help='timed solves per precision')
+    ap.add_argument('--requests', type=int, default=300, help='serving requests per rate')
+    ap.add_argument('--no-serving', action='store_true')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference_arm(args)
-    if args.only == 'poisson':
+    if args.only:
         import torch
         torch.cuda.set_device(0)
-        pb, _, _, _ = poisson_bench(args.solves)
-        print(json.dumps({'poisson': pb}))
+        if args.only == 'poisson':
+            pb, _, _, _ = poisson_bench(args.solves)
+            print(json.dumps({'poisson': pb}))
+        elif args.only == 'serving':
+            print(json.dumps({'serving': serving_bench(nreq=args.requests)}))
+        else:
+            print(json.dumps(batch_bench()))
         return 0
     return run_gpu_arm(args)
 

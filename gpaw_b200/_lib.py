@@ -63,6 +63,15 @@ SIGNATURES = {
     'gfd_poisson_destroy': (ctypes.c_int, [_vp]),
     'gfd_poisson_solve': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, _ip, _dp, _vp]),
+    'gfd_poisson_solve_async': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_int, _vp]),
+    'gfd_poisson_result': (ctypes.c_int, [_vp, _ip, _dp]),
+    'gfd_poisson_batch_create': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp),
+                                                ctypes.POINTER(_vp)]),
+    'gfd_poisson_batch_destroy': (ctypes.c_int, [_vp]),
+    'gfd_poisson_batch_solve_async': (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                                     ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                     _vp]),
     'gfd_grid_sum': (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double, _dp, _vp]),
 }
 

@@ -217,116 +217,192 @@ static int loop_body(gfd_poisson* ps, cudaGraphConditionalHandle loop, int in_gr
   return check_launch("check_kernel");
 }
 
-// Capture the solve graph: prologue, while(loop_body), epilogue.
-static int build_graph(gfd_poisson* ps) {
-  cudaStream_t cs = nullptr;
-  int st = check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
-  if (st) return st;
+// Enqueue one solver's part of a graph on a capturing stream: prologue
+// (charge, background, rho - background), a `while` conditional node and
+// the epilogue (zero-mean potential when fully periodic).  Returns the
+// loop's body graph and handle; the body is filled by capture_body once the
+// outer capture has ended.
+static int capture_solve(gfd_poisson* ps, cudaStream_t cs, cudaGraph_t* body_out,
+                         cudaGraphConditionalHandle* loop_out) {
   Level& L0 = ps->L[0];
   const int64_t n0 = L0.n;
   const int blocks = grid_for(n0);
-  cudaGraph_t graph = nullptr;
+  int st;
   cudaGraphConditionalHandle loop;
-  cudaGraphNode_t cond_node;
-  cudaGraph_t body = nullptr;
-  auto fail = [&](int code) {
-    cudaStreamCaptureStatus cst;
-    if (cudaStreamIsCapturing(cs, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
-      cudaGraph_t g = nullptr;
-      cudaStreamEndCapture(cs, &g);
-      if (g) cudaGraphDestroy(g);
-    }
-    cudaGetLastError();
-    cudaStreamDestroy(cs);
-    return code;
-  };
-  if ((st = check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal),
-                       "cudaStreamBeginCapture")))
-    return fail(st);
   {
     cudaStreamCaptureStatus cst;
     unsigned long long id;
+    cudaGraph_t g = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
-    if ((st = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, &id, &graph, &deps, &ndeps),
+    if ((st = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, &id, &g, &deps, &ndeps),
                          "cudaStreamGetCaptureInfo")))
-      return fail(st);
-    if ((st = check_cuda(cudaGraphConditionalHandleCreate(&loop, graph, 1,
-                                                          cudaGraphCondAssignDefault),
+      return st;
+    if ((st = check_cuda(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault),
                          "cudaGraphConditionalHandleCreate")))
-      return fail(st);
+      return st;
   }
-  // Prologue: charge, background, rho - background.
   if ((st = reduce_launch(GFD_FLOAT64, ps->rho_in, n0, false, ps->dv, ps->partials,
                           &ps->dctrl->charge, cs)))
-    return fail(st);
+    return st;
   launch_k(prep_kernel, 1, 1, 0, cs, ps->dctrl, double(n0), ps->dv, loop, 1);
   double* rho0 = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.rho) : ps->rho64;
-  launch_k(sub_bg_kernel, blocks, 256, 0, cs, rho0, ps->rho_in, ps->dctrl, n0);
-  if ((st = check_launch("prologue"))) return fail(st);
-  if (ps->precision == GFD_POISSON_MIXED) {
-    if ((st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1, nullptr,
-                        0.0, nullptr, cs)))
-      return fail(st);
-  }
-  // The loop node.
+  launch_k(sub_bg_kernel, blocks, 256, 0, cs, rho0, ps->rho_in, ps->dctrl, (long long)n0);
+  if ((st = check_launch("prologue"))) return st;
+  if (ps->precision == GFD_POISSON_MIXED &&
+      (st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1, nullptr,
+                      0.0, nullptr, cs)))
+    return st;
   {
     cudaStreamCaptureStatus cst;
     unsigned long long id;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
-    cudaGraph_t g2 = nullptr;
-    if ((st = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, &id, &g2, &deps, &ndeps),
+    cudaGraph_t g = nullptr;
+    if ((st = check_cuda(cudaStreamGetCaptureInfo(cs, &cst, &id, &g, &deps, &ndeps),
                          "cudaStreamGetCaptureInfo")))
-      return fail(st);
+      return st;
     cudaGraphNodeParams np = {};
     np.type = cudaGraphNodeTypeConditional;
     np.conditional.handle = loop;
     np.conditional.type = cudaGraphCondTypeWhile;
     np.conditional.size = 1;
-    if ((st = check_cuda(cudaGraphAddNode(&cond_node, g2, deps, ndeps, &np), "cudaGraphAddNode")))
-      return fail(st);
-    body = np.conditional.phGraph_out[0];
-    if ((st = check_cuda(cudaStreamUpdateCaptureDependencies(cs, &cond_node, 1,
+    cudaGraphNode_t node;
+    if ((st = check_cuda(cudaGraphAddNode(&node, g, deps, ndeps, &np), "cudaGraphAddNode")))
+      return st;
+    *body_out = np.conditional.phGraph_out[0];
+    if ((st = check_cuda(cudaStreamUpdateCaptureDependencies(cs, &node, 1,
                                                              cudaStreamSetCaptureDependencies),
                          "cudaStreamUpdateCaptureDependencies")))
-      return fail(st);
+      return st;
   }
-  // Epilogue: zero mean potential for fully periodic systems.
   double* phi_final = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.phi[0])
                                                         : ps->phi64;
   if (ps->pbc_all) {
     if ((st = reduce_launch(GFD_FLOAT64, phi_final, n0, false, 1.0, ps->partials, &ps->dctrl->sum,
                             cs)))
-      return fail(st);
-    launch_k(sub_mean_kernel, blocks, 256, 0, cs, phi_final, ps->dctrl, n0);
-    if ((st = check_launch("sub_mean_kernel"))) return fail(st);
+      return st;
+    launch_k(sub_mean_kernel, blocks, 256, 0, cs, phi_final, ps->dctrl, (long long)n0);
+    if ((st = check_launch("sub_mean_kernel"))) return st;
   }
-  if ((st = check_cuda(cudaStreamEndCapture(cs, &graph), "cudaStreamEndCapture"))) return fail(st);
-  // Populate the loop body.
-  if ((st = check_cuda(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
-                                                     cudaStreamCaptureModeThreadLocal),
-                       "cudaStreamBeginCaptureToGraph"))) {
-    cudaGraphDestroy(graph);
-    return fail(st);
-  }
+  *loop_out = loop;
+  return GFD_OK;
+}
+
+static int capture_body(gfd_poisson* ps, cudaStream_t cs, cudaGraph_t body,
+                        cudaGraphConditionalHandle loop) {
+  int st = check_cuda(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeThreadLocal),
+                      "cudaStreamBeginCaptureToGraph");
+  if (st) return st;
   st = loop_body(ps, loop, 1, cs);
-  {
-    cudaGraph_t b2 = nullptr;
-    int st2 = check_cuda(cudaStreamEndCapture(cs, &b2), "cudaStreamEndCapture(body)");
-    if (!st) st = st2;
+  cudaGraph_t b2 = nullptr;
+  int st2 = check_cuda(cudaStreamEndCapture(cs, &b2), "cudaStreamEndCapture(body)");
+  return st ? st : st2;
+}
+
+static void abort_capture(cudaStream_t cs) {
+  cudaStreamCaptureStatus cst;
+  if (cudaStreamIsCapturing(cs, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(cs, &g);
+    if (g) cudaGraphDestroy(g);
   }
+  cudaGetLastError();
+}
+
+// Capture the graphs of n solvers as independent branches of one graph (one
+// solver: that solver's own graph).
+static int build_multi_graph(gfd_poisson* const* solvers, int n, cudaGraph_t* graph_out,
+                             cudaGraphExec_t* exec_out) {
+  std::vector<cudaStream_t> cs(n + 1, nullptr);
+  for (auto& c : cs) {
+    int st = check_cuda(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (st) {
+      for (auto& d : cs) if (d) cudaStreamDestroy(d);
+      return st;
+    }
+  }
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join(n, nullptr);
+  std::vector<cudaGraph_t> bodies(n, nullptr);
+  std::vector<cudaGraphConditionalHandle> loops(n);
+  cudaGraph_t graph = nullptr;
+  int st = check_cuda(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "cudaEventCreate");
+  for (int i = 0; i < n && !st; i++)
+    st = check_cuda(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming), "cudaEventCreate");
+  cudaStream_t origin = cs[n];
+  if (!st)
+    st = check_cuda(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal),
+                    "cudaStreamBeginCapture");
+  if (!st) st = check_cuda(cudaEventRecord(fork, origin), "cudaEventRecord");
+  for (int i = 0; i < n && !st; i++) {
+    st = check_cuda(cudaStreamWaitEvent(cs[i], fork, 0), "cudaStreamWaitEvent");
+    if (!st) st = capture_solve(solvers[i], cs[i], &bodies[i], &loops[i]);
+    if (!st) st = check_cuda(cudaEventRecord(join[i], cs[i]), "cudaEventRecord");
+    if (!st) st = check_cuda(cudaStreamWaitEvent(origin, join[i], 0), "cudaStreamWaitEvent");
+  }
+  if (st) {
+    for (auto& c : cs) abort_capture(c);
+  } else {
+    st = check_cuda(cudaStreamEndCapture(origin, &graph), "cudaStreamEndCapture");
+  }
+  for (int i = 0; i < n && !st; i++) st = capture_body(solvers[i], cs[0], bodies[i], loops[i]);
   if (!st) {
     cudaGraphExec_t exec = nullptr;
     st = check_cuda(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
     if (!st) {
-      ps->graph = graph;
-      ps->exec = exec;
+      *graph_out = graph;
+      *exec_out = exec;
     }
   }
-  if (st) cudaGraphDestroy(graph);
-  cudaStreamDestroy(cs);
+  if (st && graph) cudaGraphDestroy(graph);
+  if (fork) cudaEventDestroy(fork);
+  for (auto& e : join) if (e) cudaEventDestroy(e);
+  for (auto& c : cs) cudaStreamDestroy(c);
   return st;
+}
+
+static int build_graph(gfd_poisson* ps) {
+  gfd_poisson* one[1] = {ps};
+  return build_multi_graph(one, 1, &ps->graph, &ps->exec);
+}
+
+// Copy-in of the controls, rho and phi (before a graph launch) and copy-out
+// of phi and the controls (after it); the results are read by
+// gfd_poisson_result once the stream has reached that point.
+static int stage_in(gfd_poisson* ps, double* phi, const double* rho, double charge, double eps,
+                    double maxcharge, int maxiter, cudaStream_t s) {
+  const int64_t n0 = ps->L[0].n;
+  double* phi_int = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
+                                                      : ps->phi64;
+  SolveCtrl* h = ps->hctrl;
+  h->eps = eps;
+  h->maxcharge = maxcharge;
+  h->charge_arg = charge;
+  h->maxiter = maxiter;
+  int st;
+  if ((st = check_cuda(cudaMemcpyAsync(ps->dctrl, h, offsetof(SolveCtrl, charge),
+                                       cudaMemcpyHostToDevice, s),
+                       "cudaMemcpyAsync(controls)")))
+    return st;
+  if ((st = check_cuda(cudaMemcpyAsync(ps->rho_in, rho, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                       "cudaMemcpyAsync(rho)")))
+    return st;
+  return check_cuda(cudaMemcpyAsync(phi_int, phi, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                    "cudaMemcpyAsync(phi)");
+}
+
+static int stage_out(gfd_poisson* ps, double* phi, cudaStream_t s) {
+  const int64_t n0 = ps->L[0].n;
+  double* phi_int = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
+                                                      : ps->phi64;
+  int st = check_cuda(cudaMemcpyAsync(phi, phi_int, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                      "cudaMemcpyAsync(phi)");
+  if (st) return st;
+  return check_cuda(cudaMemcpyAsync(ps->hctrl, ps->dctrl, sizeof(SolveCtrl),
+                                    cudaMemcpyDeviceToHost, s),
+                    "cudaMemcpyAsync(controls)");
 }
 
 // The solve without a graph: prologue, host-driven loop, epilogue.
@@ -498,6 +574,34 @@ extern "C" int gfd_poisson_destroy(gfd_poisson* ps) {
   return GFD_OK;
 }
 
+extern "C" int gfd_poisson_solve_async(gfd_poisson* ps, double* phi, const double* rho,
+                                       double charge, double eps, double maxcharge, int maxiter,
+                                       void* stream) {
+  if (!ps) return set_error(GFD_EINVAL, "null solver");
+  if (!phi || !rho) return set_error(GFD_EINVAL, "null array pointer");
+  if (maxiter < 1) return set_error(GFD_EINVAL, "maxiter must be >= 1");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st;
+  if (!ps->exec && (st = build_graph(ps))) return st;
+  if ((st = stage_in(ps, phi, rho, charge, eps, maxcharge, maxiter, s))) return st;
+  if ((st = check_cuda(cudaGraphLaunch(ps->exec, s), "cudaGraphLaunch"))) return st;
+  return stage_out(ps, phi, s);
+}
+
+extern "C" int gfd_poisson_result(const gfd_poisson* ps, int* niter, double* error) {
+  if (!ps) return set_error(GFD_EINVAL, "null solver");
+  const SolveCtrl* h = ps->hctrl;
+  if (h->status == GFD_EUNSUPPORTED)
+    return set_error(GFD_EUNSUPPORTED,
+                     "charged system: only the charge-neutral branch of solve() is provided");
+  if (niter) *niter = h->niter;
+  if (error) *error = h->err;
+  if (h->niter >= h->maxiter)
+    return set_error(GFD_ENOCONV, "Poisson solver did not converge in " +
+                                      std::to_string(h->maxiter) + " iterations!");
+  return GFD_OK;
+}
+
 extern "C" int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho, double charge,
                                  double eps, double maxcharge, int maxiter, int* niter_out,
                                  double* error_out, void* stream) {
@@ -505,51 +609,81 @@ extern "C" int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho
   if (!phi || !rho) return set_error(GFD_EINVAL, "null array pointer");
   if (maxiter < 1) return set_error(GFD_EINVAL, "maxiter must be >= 1");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int st;
   // GFD_POISSON_EAGER=1: the same kernels launched one by one with a host
   // loop (one wait per V-cycle), for per-kernel profiling.
   static const bool eager = [] {
     const char* e = getenv("GFD_POISSON_EAGER");
     return e && e[0] == '1';
   }();
-  if (!eager && !ps->exec && (st = build_graph(ps))) return st;
-  const int64_t n0 = ps->L[0].n;
-  double* phi_int = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
-                                                      : ps->phi64;
-  SolveCtrl* h = ps->hctrl;
-  h->eps = eps;
-  h->maxcharge = maxcharge;
-  h->charge_arg = charge;
-  h->maxiter = maxiter;
-  if ((st = check_cuda(cudaMemcpyAsync(ps->dctrl, h, offsetof(SolveCtrl, charge),
-                                       cudaMemcpyHostToDevice, s),
-                       "cudaMemcpyAsync(controls)")))
-    return st;
-  if ((st = check_cuda(cudaMemcpyAsync(ps->rho_in, rho, n0 * 8, cudaMemcpyDeviceToDevice, s),
-                       "cudaMemcpyAsync(rho)")))
-    return st;
-  if ((st = check_cuda(cudaMemcpyAsync(phi_int, phi, n0 * 8, cudaMemcpyDeviceToDevice, s),
-                       "cudaMemcpyAsync(phi)")))
-    return st;
+  int st;
   if (!eager) {
-    if ((st = check_cuda(cudaGraphLaunch(ps->exec, s), "cudaGraphLaunch"))) return st;
-  } else if ((st = solve_eager(ps, s))) {
+    if ((st = gfd_poisson_solve_async(ps, phi, rho, charge, eps, maxcharge, maxiter, stream)))
+      return st;
+  } else {
+    if ((st = stage_in(ps, phi, rho, charge, eps, maxcharge, maxiter, s))) return st;
+    if ((st = solve_eager(ps, s))) return st;
+    if ((st = stage_out(ps, phi, s))) return st;
+  }
+  if ((st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize(solve)"))) return st;
+  return gfd_poisson_result(ps, niter_out, error_out);
+}
+
+// ---------------------------------------------------------------------------
+// Batches: several solvers (any grid sizes) as parallel branches of one graph.
+// ---------------------------------------------------------------------------
+struct gfd_poisson_batch {
+  std::vector<gfd_poisson*> solvers;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solvers,
+                                        gfd_poisson_batch** out) {
+  if (!out) return set_error(GFD_EINVAL, "null output handle");
+  *out = nullptr;
+  if (nsolvers < 1 || !solvers) return set_error(GFD_EINVAL, "a batch needs at least one solver");
+  for (int i = 0; i < nsolvers; i++) {
+    if (!solvers[i]) return set_error(GFD_EINVAL, "null solver in batch");
+    for (int j = 0; j < i; j++)
+      if (solvers[j] == solvers[i])
+        return set_error(GFD_EINVAL, "a solver may appear only once in a batch");
+  }
+  gfd_poisson_batch* b = new (std::nothrow) gfd_poisson_batch();
+  if (!b) return set_error(GFD_ENOMEM, "host allocation failed");
+  b->solvers.assign(solvers, solvers + nsolvers);
+  int st = build_multi_graph(b->solvers.data(), nsolvers, &b->graph, &b->exec);
+  if (st) {
+    delete b;
     return st;
   }
-  if ((st = check_cuda(cudaMemcpyAsync(h, ps->dctrl, sizeof(SolveCtrl), cudaMemcpyDeviceToHost, s),
-                       "cudaMemcpyAsync(controls)")))
-    return st;
-  if ((st = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize(solve)"))) return st;
-  if (h->status == GFD_EUNSUPPORTED)
-    return set_error(GFD_EUNSUPPORTED,
-                     "charged system: only the charge-neutral branch of solve() is provided");
-  if (niter_out) *niter_out = h->niter;
-  if (error_out) *error_out = h->err;
-  if ((st = check_cuda(cudaMemcpyAsync(phi, phi_int, n0 * 8, cudaMemcpyDeviceToDevice, s),
-                       "cudaMemcpyAsync(phi)")))
-    return st;
-  if (h->niter >= maxiter)
-    return set_error(GFD_ENOCONV, "Poisson solver did not converge in " +
-                                      std::to_string(maxiter) + " iterations!");
+  *out = b;
+  return GFD_OK;
+}
+
+extern "C" int gfd_poisson_batch_destroy(gfd_poisson_batch* b) {
+  if (!b) return GFD_OK;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  delete b;
+  return GFD_OK;
+}
+
+extern "C" int gfd_poisson_batch_solve_async(gfd_poisson_batch* b, double* const* phis,
+                                             const double* const* rhos, double eps,
+                                             double maxcharge, int maxiter, void* stream) {
+  if (!b) return set_error(GFD_EINVAL, "null batch");
+  if (!phis || !rhos) return set_error(GFD_EINVAL, "null array list");
+  if (maxiter < 1) return set_error(GFD_EINVAL, "maxiter must be >= 1");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n = (int)b->solvers.size();
+  int st;
+  for (int i = 0; i < n; i++) {
+    if (!phis[i] || !rhos[i]) return set_error(GFD_EINVAL, "null array pointer in batch");
+    if ((st = stage_in(b->solvers[i], phis[i], rhos[i], std::nan(""), eps, maxcharge, maxiter, s)))
+      return st;
+  }
+  if ((st = check_cuda(cudaGraphLaunch(b->exec, s), "cudaGraphLaunch(batch)"))) return st;
+  for (int i = 0; i < n; i++)
+    if ((st = stage_out(b->solvers[i], phis[i], s))) return st;
   return GFD_OK;
 }

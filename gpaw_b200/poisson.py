@@ -115,14 +115,7 @@ class PoissonSolver:
         V-cycles.  Raises PoissonConvergenceError after maxiter V-cycles."""
         if self.solver is None:
             self.initialize()
-        require_device(phi, 'phi')
-        require_device(rho, 'rho')
-        import torch
-        if phi.dtype != torch.float64 or rho.dtype != torch.float64:
-            raise ValueError('phi and rho must be float64')
-        shape = tuple(int(x) for x in self.gd.n_c)
-        if tuple(phi.shape) != shape or tuple(rho.shape) != shape:
-            raise ValueError('phi and rho must have the grid shape %s' % (shape,))
+        self._check_arrays(phi, rho)
         if eps is None:
             eps = self.eps
         if zero_initial_phi:
@@ -137,6 +130,63 @@ class PoissonSolver:
         self.error = err.value
         _lib.check(status, 'PoissonSolver.solve')
         return niter.value
+
+    def prepare(self):
+        """Allocate the hierarchy and capture the solve graph now (a solve of
+        rho = 0, which stops after one V-cycle), so the first real solve
+        does not pay for them."""
+        import torch
+        if self.solver is None:
+            self.initialize()
+        z = torch.zeros(tuple(int(x) for x in self.gd.n_c), dtype=torch.float64,
+                        device=self.gd.device)
+        self.solve(z, torch.zeros_like(z))
+
+    def solve_async(self, phi, rho, charge=None, eps=None, maxcharge=1e-6):
+        """Enqueue a solve on the current stream and return at once; call
+        result() after the stream has passed it (e.g. a recorded event)."""
+        if self.solver is None:
+            self.initialize()
+        self._check_arrays(phi, rho)
+        if eps is None:
+            eps = self.eps
+        _lib.check(_lib.lib.gfd_poisson_solve_async(
+            self.solver, phi.data_ptr(), rho.data_ptr(),
+            _lib.nan() if charge is None else float(charge), float(eps), float(maxcharge),
+            int(self.maxiter), stream_of(phi)), 'PoissonSolver.solve_async')
+
+    def result(self):
+        """(niter, error) of the last completed solve_async; raises as solve."""
+        niter = _lib.ctypes.c_int(0)
+        err = _lib.ctypes.c_double(0.0)
+        status = _lib.lib.gfd_poisson_result(self.solver, _lib.ctypes.byref(niter),
+                                             _lib.ctypes.byref(err))
+        self.niter = niter.value
+        self.error = err.value
+        _lib.check(status, 'PoissonSolver.result')
+        return niter.value, err.value
+
+    def _check_arrays(self, phi, rho):
+        import torch
+        require_device(phi, 'phi')
+        require_device(rho, 'rho')
+        if phi.dtype != torch.float64 or rho.dtype != torch.float64:
+            raise ValueError('phi and rho must be float64')
+        shape = tuple(int(x) for x in self.gd.n_c)
+        if tuple(phi.shape) != shape or tuple(rho.shape) != shape:
+            raise ValueError('phi and rho must have the grid shape %s' % (shape,))
+
+    def nbytes(self):
+        """Device memory held by the solver's level hierarchy (bytes)."""
+        esz = 4 if self.precision == 'mixed' else 8
+        n = int(np.prod(self.gd.n_c))
+        total = n * 8 * (4 if self.precision == 'mixed' else 1)
+        g = self.gd
+        for level in range(self.levels + 1):
+            total += 4 * int(np.prod(g.n_c)) * esz
+            if level < self.levels:
+                g = g.coarsen()
+        return total
 
     def estimate_memory(self, mem):
         nbytes = 0

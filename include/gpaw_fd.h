@@ -188,6 +188,34 @@ GFD_API int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho, d
                       double eps, double maxcharge, int maxiter, int* niter, double* error,
                       void* stream);
 
+/* Asynchronous form of gfd_poisson_solve for callers that keep several solves
+ * in flight (serving).  Enqueues the whole solve on `stream` -- copies of
+ * phi/rho into the solver, one graph launch, copy of the result back into
+ * phi -- and returns at once.  Once the stream has passed that point (an
+ * event or a synchronisation), gfd_poisson_result gives the V-cycle count,
+ * the last residual norm and the status gfd_poisson_solve would have
+ * returned.  A solver runs one solve at a time: do not enqueue a second solve
+ * on the same solver before the first has completed.  (The reference's solve
+ * is synchronous; this split has no counterpart there.) */
+GFD_API int gfd_poisson_solve_async(gfd_poisson* ps, double* phi, const double* rho, double charge,
+                                    double eps, double maxcharge, int maxiter, void* stream);
+GFD_API int gfd_poisson_result(const gfd_poisson* ps, int* niter, double* error);
+
+/* Batch of independent solvers (any grid sizes, one solver at most once),
+ * captured as parallel branches of a single CUDA graph: one launch runs every
+ * solve's V-cycle loop concurrently on the device, each stopping on its own
+ * criterion.  phis[i] / rhos[i] belong to solvers[i]; results per solver via
+ * gfd_poisson_result.  Each solver keeps its own buffers, so a solver must not
+ * run in two batches, or in a batch and a single solve, at the same time.
+ * (No counterpart in the reference, which solves one grid per call.) */
+typedef struct gfd_poisson_batch gfd_poisson_batch;
+GFD_API int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solvers,
+                                     gfd_poisson_batch** batch);
+GFD_API int gfd_poisson_batch_destroy(gfd_poisson_batch* batch);
+GFD_API int gfd_poisson_batch_solve_async(gfd_poisson_batch* batch, double* const* phis,
+                                          const double* const* rhos, double eps, double maxcharge,
+                                          int maxiter, void* stream);
+
 /* ------------------------------------------------------------------------
  * Reductions.
  * sum over all points of a float64 array of n elements, times scale (the
