@@ -11,6 +11,7 @@ process (for example PyTorch) loaded.
 import argparse
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -39,17 +40,27 @@ def _sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith('.cu'))
 
 
-def _headers_mtime():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cuh', '.h'))]
-    hs.append(os.path.join(INCLUDE, 'gpaw_fd.h'))
-    return max(os.path.getmtime(h) for h in hs)
+def _local_includes(path, seen):
+    """Headers of this package that `path` includes, transitively."""
+    for line in open(path):
+        m = re.match(r'\s*#\s*include\s+"([^"]+)"', line)
+        if not m:
+            continue
+        for d in (CSRC, INCLUDE):
+            h = os.path.join(d, m.group(1))
+            if os.path.exists(h) and h not in seen:
+                seen.add(h)
+                _local_includes(h, seen)
+                break
+    return seen
 
 
 def _compile(src, force, ptxas_verbose):
     obj = os.path.join(BUILD, src[:-3] + '.o')
     srcp = os.path.join(CSRC, src)
+    deps = [srcp] + sorted(_local_includes(srcp, set()))
     if (not force and os.path.exists(obj) and
-            os.path.getmtime(obj) >= max(os.path.getmtime(srcp), _headers_mtime())):
+            os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps)):
         return obj, ''
     cmd = [nvcc()] + ARCH + NVCC_FLAGS + ['-c', srcp, '-o', obj]
     if ptxas_verbose:

@@ -4,9 +4,11 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "internal.h"
 #include "stencil.cuh"
+#include "stencil_tma.cuh"
 
 namespace gfd {
 
@@ -149,6 +151,63 @@ int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V
   return set_error(GFD_EUNSUPPORTED, "star stencil radius out of range");
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed kernel (stencil_tma.cuh): complex128 apply on grids whose plane
+// holds whole 16 x 32 tiles along periodic axes (zero-boundary axes may end
+// in a partial tile: the loads fill zeros past the edge).
+// ---------------------------------------------------------------------------
+constexpr int kTmaVY = 2, kTmaG = 8, kTmaBY = kTmaVY * kTmaG, kTmaStages = 8;
+
+// Defined in operator.cu.
+bool star_tma_enabled();
+int* star_error_flag();
+int encode_tma_maps(TmaMaps* maps, const void* base, const gfd_operator* op, int64_t nb, int R,
+                    int by);
+
+inline bool tma_eligible(const gfd_operator* op, const void* in) {
+  if (!star_tma_enabled() || op->R < 1 || op->R > 3) return false;
+  if (op->n[2] < kTmaBZ || op->n[1] < kTmaBY) return false;
+  if (op->per[2] && op->n[2] % kTmaBZ) return false;
+  if (op->per[1] && op->n[1] % kTmaBY) return false;
+  return (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+}
+
+template <int R>
+int star_tma_go(const gfd_operator* op, const cplx<double>* in, cplx<double>* out, int64_t nin,
+                const StarParams<double>& base, const LaunchGeom& g, cudaStream_t s) {
+  constexpr size_t smem = star_tma_smem_bytes<R, kTmaBY, kTmaStages>();
+  auto kern = star_tma_kernel<R, kTmaVY, kTmaG, kTmaStages>;
+  int st = raise_smem_limit(kern, smem, "cudaFuncSetAttribute(star_tma_kernel)");
+  if (st) return st;
+  // Two CTAs per SM need the largest shared-memory carveout.
+  if ((st = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            int(cudaSharedmemCarveoutMaxShared)),
+                       "cudaFuncSetAttribute(carveout)")))
+    return st;
+  int* err = star_error_flag();
+  if (!err) return GFD_ECUDA;
+  TmaMaps maps;
+  if ((st = encode_tma_maps(&maps, in, op, nin, R, kTmaBY))) return st;
+  const long long band = (long long)op->n[0] * op->n[1] * op->n[2];
+  for (int64_t b0 = 0; b0 < nin; b0 += g.bands_per_launch) {
+    int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
+    dim3 grid(g.grid.x, g.grid.y, (unsigned)(nb * g.nxc));
+    launch_k(kern, grid, 32 * kTmaG, smem, s, out + b0 * band, base, maps, (int)b0, err);
+  }
+  return check_launch("star_tma_kernel");
+}
+
+inline int star_tma_dispatch(const gfd_operator* op, const cplx<double>* in, cplx<double>* out,
+                             int64_t nin, const StarParams<double>& p, const LaunchGeom& g,
+                             cudaStream_t s) {
+  switch (op->R) {
+    case 1: return star_tma_go<1>(op, in, out, nin, p, g, s);
+    case 2: return star_tma_go<2>(op, in, out, nin, p, g, s);
+    case 3: return star_tma_go<3>(op, in, out, nin, p, g, s);
+  }
+  return set_error(GFD_EUNSUPPORTED, "TMA stencil radius out of range");
+}
+
 template <class V, int MODE>
 int direct_dispatch(const gfd_operator* op, const V* in, V* out, const V* rho,
                     const StarParams<typename vt<V>::S>& p, long long total, cudaStream_t s) {
@@ -207,6 +266,14 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
         return direct_dispatch<V, MODE_RESIDUAL>(op, vin, vout, vrho, p, total, s);
     }
     return direct_dispatch<V, MODE_APPLY>(op, vin, vout, nullptr, p, total, s);
+  }
+  if constexpr (std::is_same_v<V, cplx<double>>) {
+    if (mode == OP_APPLY && tma_eligible(op, in)) {
+      LaunchGeom g = star_geom(op, TILE_WIDE, nin, op->R);
+      p.nxc = g.nxc;
+      p.x_chunk = g.x_chunk;
+      return star_tma_dispatch(op, vin, vout, nin, p, g, s);
+    }
   }
   const int tile = pick_tile(op);
   LaunchGeom g = star_geom(op, tile, nin, op->R);

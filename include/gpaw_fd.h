@@ -133,6 +133,12 @@ GFD_API int gfd_operator_relax_noalloc(gfd_operator* op, int dtype, int relax_me
  * c/operators.c:408-421). */
 GFD_API int gfd_operator_get_diagonal_element(const gfd_operator* op, double* d);
 
+/* Device-side error flags of the current device, then cleared: *flags != 0
+ * when a stencil kernel gave up on a bounded wait since the last call (its
+ * output is then incomplete).  No counterpart in the reference, whose CPU
+ * kernels have no such waits. */
+GFD_API int gfd_device_errors(int* flags);
+
 /* ------------------------------------------------------------------------
  * Grid transformer (restriction / interpolation).
  * Replaces _gpaw.Transformer(size_in, size_out, k, paddings, npaddings,

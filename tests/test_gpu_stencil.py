@@ -208,3 +208,83 @@ def test_multicolour_gauss_seidel(golden, cuda, tag):
     ref = multicolour_gs_reference(c, o, gd.pbc_c, d['relax_%s_phi0' % tag],
                                    d['relax_%s_rho' % tag], 2)
     assert rel_err(host(phi), ref) < TOL
+
+
+BLOCKED_SHAPES = [((24, 16, 33), 1), ((40, 20, 36), 1), ((40, 20, 36), 0), ((17, 18, 40), (0, 1, 1)),
+                  ((9, 33, 64), (1, 1, 0))]
+
+
+@pytest.mark.parametrize('N,pbc', BLOCKED_SHAPES)
+@pytest.mark.parametrize('n', [1, 2, 3])
+def test_register_blocked_tiles(cuda, N, pbc, n):
+    """Grids at least 16 x 32 in the plane (the register-blocked kernel for
+    8- and 16-byte values): partial tiles, halos wrapping more than once on a
+    narrow periodic axis, Bloch phases on every axis; float64, complex128 and
+    complex64, and weighted-Jacobi sweeps."""
+    import torch
+    from gpaw_b200.fd_operators import FDOperator
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    gd = G.Grid(N, np.array(N) * 0.3, pbc)
+    c, o = G.laplace_stencil(gd, -0.5, n)
+    rng = np.random.default_rng(10 + n)
+    a = rng.standard_normal((3,) + tuple(gd.n_c))
+    args = (gd.N_c, gd.cell_cv, gd.pbc_c)
+    assert rel_err(gpu_apply(cuda, args, c, o, a), K.fd_apply(c, o, gd.pbc_c, a)) < TOL
+    ac = a + 1j * rng.standard_normal(a.shape)
+    ph = G.bloch_phases(gd, (0.3, -0.2, 0.15))
+    ref = K.fd_apply(c, o, gd.pbc_c, ac, ph)
+    assert rel_err(gpu_apply(cuda, args, c, o, ac, ph), ref) < TOL
+    o64 = gpu_apply(cuda, args, c, o, ac, ph, dtype=torch.complex64)
+    assert rel_err(o64.astype(complex), ref) < 2e-6
+    # three weighted-Jacobi sweeps on one band
+    op = FDOperator(c, o, GridDescriptor(*args))
+    phi0, rho = a[0], a[1]
+    phi = dev(phi0, cuda)
+    op.relax(2, phi, dev(rho, cuda), 3, 2.0 / 3.0)
+    p = phi0.copy()
+    K.relax(2, c, o, gd.pbc_c, p, rho, 3, 2.0 / 3.0)
+    assert rel_err(host(phi), p) < TOL
+
+
+TMA_SHAPES = [((40, 32, 64), 1), ((24, 48, 96), (1, 1, 0)), ((20, 16, 32), (0, 1, 1)),
+              ((18, 37, 70), 0), ((96, 96, 96), 1)]
+
+
+@pytest.mark.parametrize('N,pbc', TMA_SHAPES)
+@pytest.mark.parametrize('n', [1, 2, 3])
+def test_complex128_tiles_all_boundaries(cuda, N, pbc, n):
+    """complex128 bands on grids of whole 16 x 32 plane tiles along periodic
+    axes (and ragged zero-boundary axes): Bloch phases on all three axes,
+    Laplace and a gradient, then the device error flags stay clear."""
+    import ctypes
+    from gpaw_b200 import _lib
+    gd = G.Grid(N, np.array(N) * 0.3, pbc)
+    rng = np.random.default_rng(20 + n)
+    nb = 2 if N[0] < 96 else 1
+    a = rng.standard_normal((nb,) + tuple(gd.n_c)) + 1j * rng.standard_normal((nb,) + tuple(gd.n_c))
+    args = (gd.N_c, gd.cell_cv, gd.pbc_c)
+    for k in ((0.3, -0.2, 0.15), (0.25, 0.0, 0.0)):
+        ph = G.bloch_phases(gd, k)
+        for c, o in (G.laplace_stencil(gd, -0.5, n), G.gradient_stencil(gd, 2, 1.0, n)):
+            ref = K.fd_apply(c, o, gd.pbc_c, a, ph, nthreads=8)
+            assert rel_err(gpu_apply(cuda, args, c, o, a, ph), ref) < TOL, k
+    flags = ctypes.c_int(-1)
+    assert _lib.lib.gfd_device_errors(ctypes.byref(flags)) == 0
+    assert flags.value == 0
+
+
+def test_tma_fed_kernel_in_subprocess(cuda):
+    """The TMA-fed complex128 kernel (opt-in with GFD_STAR_TMA=1, read once
+    per process) against the oracle: the tile tests above in a child process
+    with the switch on."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, GFD_STAR_TMA='1')
+    r = subprocess.run([sys.executable, '-m', 'pytest', '-q', '-m', 'gpu', '-p', 'no:cacheprovider',
+                        os.path.join(root, 'tests', 'test_gpu_stencil.py'),
+                        '-k', 'complex128_tiles or bloch_complex_96'],
+                       cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert ' passed' in r.stdout
