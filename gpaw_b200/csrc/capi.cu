@@ -38,6 +38,17 @@ bool pdl_enabled() {
   return on;
 }
 
+// Grids up to 300000 points (all bands) use the one-thread-per-point
+// kernels, whose whole grid is in flight at once; larger ones the marching
+// kernels.  GFD_DIRECT_MAX in the environment overrides the limit.
+long long direct_max_points() {
+  static const long long v = [] {
+    const char* e = getenv("GFD_DIRECT_MAX");
+    return e ? atoll(e) : 300000LL;
+  }();
+  return v;
+}
+
 int zero_launch(int dtype, void* y, int64_t n, cudaStream_t s) {
   const int blocks = grid_for(n);
   if (dtype == GFD_FLOAT64)
@@ -121,14 +132,16 @@ int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cud
   return check_launch("sub_const_kernel");
 }
 
-int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s) {
+int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s,
+                   void* seed, double seed_scale) {
   const int blocks = grid_for(n);
   if (ydtype == GFD_FLOAT32 && xdtype == GFD_FLOAT64)
     launch_k(convert_kernel<float, double>, blocks, 256, 0, s, static_cast<float*>(y),
-                                                         static_cast<const double*>(x), n);
+             static_cast<const double*>(x), (long long)n, static_cast<float*>(seed),
+             float(seed_scale));
   else if (ydtype == GFD_FLOAT64 && xdtype == GFD_FLOAT32)
     launch_k(convert_kernel<double, float>, blocks, 256, 0, s, static_cast<double*>(y),
-                                                         static_cast<const float*>(x), n);
+             static_cast<const float*>(x), (long long)n, static_cast<double*>(seed), seed_scale);
   else
     return set_error(GFD_EINVAL, "convert: unsupported dtype pair");
   return check_launch("convert_kernel");

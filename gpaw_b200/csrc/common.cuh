@@ -138,6 +138,8 @@ __device__ __forceinline__ void pdl_enter() {
 }
 
 bool pdl_enabled();
+// Largest grid (points over all bands) for the one-thread-per-point kernels.
+long long direct_max_points();
 
 // Launch with the programmatic-stream-serialisation attribute (when
 // enabled; GFD_PDL=0 in the environment turns it off).

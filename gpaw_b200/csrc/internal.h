@@ -64,6 +64,10 @@ int op_gs_colors(const gfd_operator* op);
 
 int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,
               const double* phases, cudaStream_t s);
+// Restriction of one real band that also writes seed = seed_scale * out
+// (the first weighted-Jacobi sweep of the coarse level from a zero guess).
+int tr_launch_seed(const gfd_transformer* tr, int dtype, const void* in, void* out, void* seed,
+                   double seed_scale, cudaStream_t s);
 // Interpolation with the correction fused: out = base - interpolate(in)
 // (in place when base == out).
 int tr_launch_sub(const gfd_transformer* tr, int dtype, const void* in, void* out,
@@ -79,7 +83,9 @@ int final_sum_launch(const double* partials, int n, double scale, double* result
 int axpby_launch(int ydtype, void* y, int xdtype, const void* x, double a, double b, int64_t n,
                  cudaStream_t s);
 int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cudaStream_t s);
-int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s);
+// y = convert(x); with seed != nullptr also seed = seed_scale * y.
+int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s,
+                   void* seed = nullptr, double seed_scale = 0.0);
 int zero_launch(int dtype, void* y, int64_t n, cudaStream_t s);
 
 }  // namespace gfd

@@ -142,32 +142,60 @@ static int relax_level(gfd_poisson* ps, Level& lv, int& cur, int nsweeps, cudaSt
   return GFD_OK;
 }
 
+// A level whose correction starts from zero can take its first weighted-
+// Jacobi sweep, (w / c0) rho, from the kernel that writes its rho (seeded
+// restriction or conversion): exactly the sweep's result, one pass less.
+// Only the level's first relaxation acts on the zero guess: the
+// pre-smoothing, or on the coarsest level (which has no pre-smoothing) the
+// post-smoothing.
+static bool seedable(const gfd_poisson* ps, int l) {
+  const Level& lv = ps->L[l];
+  return ps->relax_method != GFD_RELAX_GS && lv.op->star && lv.w != 0.0 &&
+         (l < ps->levels ? lv.pre > 0 : lv.post > 0);
+}
+static double seed_scale(const Level& lv) { return lv.w / lv.op->c0; }
+
 // Enqueue one V-cycle from level l down; every level starts in phi[0] and
 // ends there.  final_norm: the level-0 residual norm into dctrl->err.
-static int iterate2(gfd_poisson* ps, int l, bool final_norm, cudaStream_t s) {
+// seeded: the level's first sweep is done already (phi[1] = (w/c0) rho from
+// a zero guess).
+static int iterate2(gfd_poisson* ps, int l, bool final_norm, cudaStream_t s,
+                    bool seeded = false) {
   Level& lv = ps->L[l];
   const size_t esz = dtype_size(ps->vdtype);
-  int cur = 0;
+  int cur = seeded ? 1 : 0;
+  int pre = lv.pre, post = lv.post;
+  if (seeded) {
+    if (l < ps->levels) pre--;
+    else post--;
+  }
   int st;
   if (l < ps->levels) {
     Level& nx = ps->L[l + 1];
-    if ((st = relax_level(ps, lv, cur, lv.pre, s))) return st;
+    if ((st = relax_level(ps, lv, cur, pre, s))) return st;
     if ((st = op_launch(lv.op, ps->vdtype, OP_RESIDUAL, lv.phi[cur], lv.res, lv.rho, 1, nullptr,
                         0.0, nullptr, s)))
       return st;
-    if ((st = tr_launch(ps->restr[l], ps->vdtype, lv.res, nx.rho, 1, nullptr, s))) return st;
-    if ((st = zero_launch(ps->vdtype, nx.phi[0], nx.n, s))) return st;
-    if ((st = iterate2(ps, l + 1, false, s))) return st;
+    const bool seed = seedable(ps, l + 1);
+    if (seed) {
+      if ((st = tr_launch_seed(ps->restr[l], ps->vdtype, lv.res, nx.rho, nx.phi[1],
+                               seed_scale(nx), s)))
+        return st;
+    } else {
+      if ((st = tr_launch(ps->restr[l], ps->vdtype, lv.res, nx.rho, 1, nullptr, s))) return st;
+      if ((st = zero_launch(ps->vdtype, nx.phi[0], nx.n, s))) return st;
+    }
+    if ((st = iterate2(ps, l + 1, false, s, seed))) return st;
     // phi -= interpolate(e): out of place when the sweeps left level l in an
     // odd position, so the post-smoothing ends in phi[0].
-    const bool flip = ((lv.post & 1) != 0) != (cur != 0) && ps->relax_method != GFD_RELAX_GS;
+    const bool flip = ((post & 1) != 0) != (cur != 0) && ps->relax_method != GFD_RELAX_GS;
     const int dst = flip ? 1 - cur : cur;
     if ((st = tr_launch_sub(ps->interp[l], ps->vdtype, nx.phi[0], lv.phi[dst], lv.phi[cur], 1,
                             nullptr, s)))
       return st;
     cur = dst;
   }
-  if ((st = relax_level(ps, lv, cur, lv.post, s))) return st;
+  if ((st = relax_level(ps, lv, cur, post, s))) return st;
   if (cur != 0) {
     // Only reachable for an odd total sweep count on a level without the
     // flip (possible with custom smoothing counts): copy back to phi[0].
@@ -200,9 +228,16 @@ static int loop_body(gfd_poisson* ps, cudaGraphConditionalHandle loop, int in_gr
   } else {
     // rho_V = float(L phi - rho); e = 0; one float32 V-cycle; phi -= e;
     // r = L phi - rho with its norm.
-    if ((st = convert_launch(GFD_FLOAT32, L0.rho, GFD_FLOAT64, ps->r64, n0, s))) return st;
-    if ((st = zero_launch(GFD_FLOAT32, L0.phi[0], n0, s))) return st;
-    if ((st = iterate2(ps, 0, false, s))) return st;
+    const bool seed = seedable(ps, 0);
+    if (seed) {
+      if ((st = convert_launch(GFD_FLOAT32, L0.rho, GFD_FLOAT64, ps->r64, n0, s, L0.phi[1],
+                               seed_scale(L0))))
+        return st;
+    } else {
+      if ((st = convert_launch(GFD_FLOAT32, L0.rho, GFD_FLOAT64, ps->r64, n0, s))) return st;
+      if ((st = zero_launch(GFD_FLOAT32, L0.phi[0], n0, s))) return st;
+    }
+    if ((st = iterate2(ps, 0, false, s, seed))) return st;
     if ((st = axpby_launch(GFD_FLOAT64, ps->phi64, GFD_FLOAT32, L0.phi[0], 1.0, -1.0, n0, s)))
       return st;
     if ((st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1,

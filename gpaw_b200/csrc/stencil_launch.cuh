@@ -37,12 +37,10 @@ inline TileDims tile_dims(int tile) {
 
 constexpr int kStages = 4;
 
-// Grids up to this many points (all bands) use the one-thread-per-point
+// Grids up to direct_max_points() (all bands) use the one-thread-per-point
 // kernel: the marching kernel's plane pipeline only pays off on larger grids.
-constexpr long long kDirectMaxPoints = 300000;
-
 inline bool use_direct(const gfd_operator* op, int64_t nin) {
-  return (long long)op->n[0] * op->n[1] * op->n[2] * nin <= kDirectMaxPoints;
+  return (long long)op->n[0] * op->n[1] * op->n[2] * nin <= direct_max_points();
 }
 inline int direct_blocks(long long total) {
   long long b = (total + 255) / 256;

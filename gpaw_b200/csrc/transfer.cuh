@@ -65,6 +65,12 @@ struct TrParams {
   int x_chunk, nxc;    // output planes per CTA along axis 0, chunk count
   long long band_in, band_out;
   Phases<S> P;
+  // Restriction only: when seed != nullptr, also write seed = seed_scale *
+  // out (same layout as out).  A weighted-Jacobi sweep from a zero guess
+  // gives exactly (w / c0) rho, so a multigrid level's first sweep comes
+  // out of the restriction that produces its rho.
+  void* seed;
+  S seed_scale;
 };
 
 // Pack an in-plane source offset and its wrap sides; -1 = zero point.
@@ -190,7 +196,9 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
           const int y = Y0 + ty + j * TYC, z = Z0 + tz;
           if (y < p.no1 && z < p.no2) {
             V v = rst_tap<NN, V>([&](int o) { return q[j][W + o]; });
-            stcs(outb + X * plane_out + (long long)y * p.no2 + z, v);
+            const long long o = X * plane_out + (long long)y * p.no2 + z;
+            stcs(outb + o, v);
+            if (p.seed) stcs(static_cast<V*>(p.seed) + (outb - out) + o, vmul(p.seed_scale, v));
           }
         }
       }
@@ -362,11 +370,13 @@ restrict_direct_kernel(const V* __restrict__ in, V* __restrict__ out,
     const V* base = in + b * p.band_in;
     // fine centre of each axis: 2i + (2nn-1) - lo
     const int fx = 2 * X + W - p.lo0, fy = 2 * Y + W - p.lo1, fz = 2 * Z + W - p.lo2;
-    out[g] = rst_tap<NN, V>([&](int ox) {
+    const V v = rst_tap<NN, V>([&](int ox) {
       return rst_tap<NN, V>([&](int oy) {
         return rst_tap<NN, V>([&](int oz) { return tr_fetch(base, fx + ox, fy + oy, fz + oz, p); });
       });
     });
+    out[g] = v;
+    if (p.seed) static_cast<V*>(p.seed)[g] = vmul(p.seed_scale, v);
   }
 }
 

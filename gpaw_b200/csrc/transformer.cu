@@ -72,9 +72,8 @@ static int interp_go(const gfd_transformer* tr, const V* in, V* out, const V* ba
   return check_launch("interp_kernel");
 }
 
-// Outputs (all bands) up to this count use the one-thread-per-point forms.
-constexpr long long kTrDirectMaxPoints = 300000;
-
+// Outputs (all bands) up to direct_max_points() use the one-thread-per-point
+// forms.
 template <class V, int NN>
 static int direct_go(const gfd_transformer* tr, const V* in, V* out, const V* base, int64_t nin,
                      const TrParams<typename vt<V>::S>& p, cudaStream_t s) {
@@ -92,7 +91,8 @@ static int direct_go(const gfd_transformer* tr, const V* in, V* out, const V* ba
 
 template <class V>
 static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const void* base_v,
-                    int64_t nin, const double* ph, cudaStream_t s) {
+                    int64_t nin, const double* ph, cudaStream_t s, void* seed = nullptr,
+                    double seed_scale = 0.0) {
   using S = typename vt<V>::S;
   TrParams<S> p{};
   p.ni0 = tr->nin[0]; p.ni1 = tr->nin[1]; p.ni2 = tr->nin[2];
@@ -103,12 +103,15 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const 
   p.band_in = (long long)tr->nin[0] * tr->nin[1] * tr->nin[2];
   p.band_out = (long long)tr->nout[0] * tr->nout[1] * tr->nout[2];
   fill_tr_phases(p.P, ph);
+  p.seed = seed;
+  p.seed_scale = S(seed_scale);
+  if (seed && tr->interpolate) return set_error(GFD_EINVAL, "seeded form is for restriction only");
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
   const V* base = static_cast<const V*>(base_v);
   if (base && !tr->interpolate)
     return set_error(GFD_EINVAL, "subtracting form is for interpolation only");
-  if (p.band_out * nin <= kTrDirectMaxPoints) {
+  if (p.band_out * nin <= direct_max_points()) {
     switch (tr->nn) {
       case 1: return direct_go<V, 1>(tr, vin, vout, base, nin, p, s);
       case 2: return direct_go<V, 2>(tr, vin, vout, base, nin, p, s);
@@ -145,6 +148,15 @@ int tr_launch_sub(const gfd_transformer* tr, int dtype, const void* in, void* ou
     case GFD_COMPLEX64: return tr_typed<cplx<float>>(tr, in, out, base, nin, phases, s);
   }
   return set_error(GFD_EINVAL, "unknown dtype");
+}
+
+int tr_launch_seed(const gfd_transformer* tr, int dtype, const void* in, void* out, void* seed,
+                   double seed_scale, cudaStream_t s) {
+  switch (dtype) {
+    case GFD_FLOAT64: return tr_typed<double>(tr, in, out, nullptr, 1, nullptr, s, seed, seed_scale);
+    case GFD_FLOAT32: return tr_typed<float>(tr, in, out, nullptr, 1, nullptr, s, seed, seed_scale);
+  }
+  return set_error(GFD_EINVAL, "seeded restriction needs a real dtype");
 }
 
 int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,

@@ -44,11 +44,15 @@ __global__ void __launch_bounds__(256) zero_kernel(T* __restrict__ y, long long 
 // y[i] = T(x[i])
 template <class Y, class X>
 __global__ void __launch_bounds__(256) convert_kernel(Y* __restrict__ y, const X* __restrict__ x,
-                                                      long long n) {
+                                                      long long n, Y* __restrict__ seed,
+                                                      Y seed_scale) {
   pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    y[i] = Y(x[i]);
+       i += (long long)gridDim.x * blockDim.x) {
+    const Y v = Y(x[i]);
+    y[i] = v;
+    if (seed) seed[i] = seed_scale * v;
+  }
 }
 
 // Per-block partial sums of a[i] (SQUARE: a[i]^2), in a fixed order.
