@@ -391,6 +391,44 @@ def batch_bench():
 
 
 # ---------------------------------------------------------------------------
+# Pseudo-Hamiltonian on the headline bands: kin psit + vt psit fused in one
+# pass against the reference's two passes (kinetic apply, then
+# Htpsit += psit * vt as a separate elementwise update).
+# ---------------------------------------------------------------------------
+def hamiltonian_bench(lap, a, b, phase, steps):
+    import torch
+    g = torch.Generator(device='cuda')
+    g.manual_seed(9)
+    vt = torch.rand(tuple(a.shape[1:]), dtype=torch.float64, device='cuda', generator=g) - 0.5
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def two_pass():
+        lap.apply(a, b, phase)
+        b.addcmul_(a, vt)
+
+    fused_ms = timed(lambda: lap.apply_with_potential(a, b, vt, phase))
+    two_ms = timed(two_pass)
+    nbytes = BYTES_PER_POINT * a.numel()
+    return {'workload': 'kin psit + vt psit, %d complex128 bands x %d^3, k=(0.25,0,0)'
+                        % (a.shape[0], a.shape[1]),
+            'fused_ms': fused_ms, 'fused_GBps': nbytes / (fused_ms * 1e-3) / 1e9,
+            'two_pass_ms': two_ms, 'speedup_vs_two_pass': two_ms / fused_ms,
+            'bytes_per_point': BYTES_PER_POINT}
+
+
+# ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args):
@@ -457,6 +495,10 @@ def run_gpu_arm(args):
                'd2h_bytes_per_step': nbytes // 2}
         del host_in, host_out
 
+    ham = None
+    if rank == 0 and world == 1 and not args.no_hamiltonian:
+        ham = hamiltonian_bench(lap, a, b, phase, min(args.steps, 20))
+
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic()
     line = {'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world,
@@ -471,6 +513,8 @@ def run_gpu_arm(args):
             'e2e': e2e,
             'gpu_launches': args.steps,
             'clocks': clocks.result()}
+    if ham is not None:
+        line['hamiltonian'] = ham
     if rank == 0 and world == 1 and not args.no_poisson:
         try:
             pb, _, _, _ = poisson_bench()
@@ -515,6 +559,7 @@ def main():
     ap.add_argument('--solves', type=int, default=8, help='timed solves per precision')
     ap.add_argument('--requests', type=int, default=300, help='serving requests per rate')
     ap.add_argument('--no-serving', action='store_true')
+    ap.add_argument('--no-hamiltonian', action='store_true')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference_arm(args)

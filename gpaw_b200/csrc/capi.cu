@@ -49,6 +49,15 @@ long long direct_max_points() {
   return v;
 }
 
+int march_ctas_per_sm() {
+  static const int v = [] {
+    const char* e = getenv("GFD_MARCH_CTAS_PER_SM");
+    const int x = e ? atoi(e) : 4;
+    return x < 1 ? 1 : (x > 64 ? 64 : x);
+  }();
+  return v;
+}
+
 int zero_launch(int dtype, void* y, int64_t n, cudaStream_t s) {
   const int blocks = grid_for(n);
   if (dtype == GFD_FLOAT64)
@@ -130,6 +139,35 @@ int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cud
   else
     return set_error(GFD_EINVAL, "sub_const: unsupported dtype");
   return check_launch("sub_const_kernel");
+}
+
+int add_potential_launch(int dtype, void* out, const void* in, const void* v, int64_t n,
+                         int64_t nin, cudaStream_t s) {
+  const long long total = (long long)n * nin;
+  const int blocks = grid_for(total);
+  switch (dtype) {
+    case GFD_FLOAT64:
+      launch_k(add_potential_kernel<double>, blocks, 256, 0, s, static_cast<double*>(out),
+               static_cast<const double*>(in), static_cast<const double*>(v), (long long)n, total);
+      break;
+    case GFD_FLOAT32:
+      launch_k(add_potential_kernel<float>, blocks, 256, 0, s, static_cast<float*>(out),
+               static_cast<const float*>(in), static_cast<const float*>(v), (long long)n, total);
+      break;
+    case GFD_COMPLEX128:
+      launch_k(add_potential_kernel<cplx<double>>, blocks, 256, 0, s,
+               static_cast<cplx<double>*>(out), static_cast<const cplx<double>*>(in),
+               static_cast<const double*>(v), (long long)n, total);
+      break;
+    case GFD_COMPLEX64:
+      launch_k(add_potential_kernel<cplx<float>>, blocks, 256, 0, s,
+               static_cast<cplx<float>*>(out), static_cast<const cplx<float>*>(in),
+               static_cast<const float*>(v), (long long)n, total);
+      break;
+    default:
+      return set_error(GFD_EINVAL, "unknown dtype");
+  }
+  return check_launch("add_potential_kernel");
 }
 
 int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s,

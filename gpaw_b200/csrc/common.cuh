@@ -140,6 +140,9 @@ __device__ __forceinline__ void pdl_enter() {
 bool pdl_enabled();
 // Largest grid (points over all bands) for the one-thread-per-point kernels.
 long long direct_max_points();
+// CTAs per SM the marching kernels aim for when they split axis 0 into
+// chunks (GFD_MARCH_CTAS_PER_SM, default 4).
+int march_ctas_per_sm();
 
 // Launch with the programmatic-stream-serialisation attribute (when
 // enabled; GFD_PDL=0 in the environment turns it off).

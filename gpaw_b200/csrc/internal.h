@@ -43,13 +43,15 @@ struct gfd_transformer {
 
 namespace gfd {
 
-enum { OP_APPLY = 0, OP_JACOBI = 1, OP_RESIDUAL = 2 };
+enum { OP_APPLY = 0, OP_JACOBI = 1, OP_RESIDUAL = 2, OP_POTENTIAL = 3 };
 
 int num_sms();
 
 // Stencil launch.  mode OP_APPLY: out = L in.  OP_JACOBI: out = Jacobi update
 // of in with source rho and weight w.  OP_RESIDUAL: out = L in - rho and, if
 // partials != nullptr, one sum of squares per CTA into partials.
+// OP_POTENTIAL (star operators only): out = L in + v in with the real grid v
+// (float64 for float64/complex128 bands, float32 otherwise) passed as rho.
 // in/out/rho point to nin bands.  phase_cd: 12 doubles (host) or nullptr.
 int op_launch(const gfd_operator* op, int dtype, int mode, const void* in, void* out,
               const void* rho, int64_t nin, const double* phase_cd, double w,
@@ -87,5 +89,9 @@ int sub_const_launch(int dtype, void* y, const void* x, double c, int64_t n, cud
 int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cudaStream_t s,
                    void* seed = nullptr, double seed_scale = 0.0);
 int zero_launch(int dtype, void* y, int64_t n, cudaStream_t s);
+// out[b][i] += v[i] * in[b][i] over nin bands of n points (v real: float64
+// for float64/complex128, float32 otherwise).
+int add_potential_launch(int dtype, void* out, const void* in, const void* v, int64_t n,
+                         int64_t nin, cudaStream_t s);
 
 }  // namespace gfd

@@ -297,6 +297,25 @@ extern "C" int gfd_operator_apply(gfd_operator* op, int dtype, const void* in, v
                    static_cast<cudaStream_t>(stream));
 }
 
+extern "C" int gfd_operator_apply_potential(gfd_operator* op, int dtype, const void* in,
+                                            void* out, int64_t nin, const double* phase_cd,
+                                            const void* v, void* stream) {
+  if (!op) return set_error(GFD_EINVAL, "null operator");
+  int st = check_dtype(op, dtype);
+  if (st) return st;
+  if (nin < 0) return set_error(GFD_EINVAL, "negative band count");
+  if (nin == 0) return GFD_OK;
+  if (!in || !out || !v) return set_error(GFD_EINVAL, "null array pointer");
+  if (in == out) return set_error(GFD_EINVAL, "input and output must not overlap");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (op->star)
+    return op_launch(op, dtype, OP_POTENTIAL, in, out, v, nin, phase_cd, 0.0, nullptr, s);
+  // Other offset sets: the stencil, then the potential term in a second pass.
+  if ((st = op_launch(op, dtype, OP_APPLY, in, out, nullptr, nin, phase_cd, 0.0, nullptr, s)))
+    return st;
+  return add_potential_launch(dtype, out, in, v, (int64_t)op->n[0] * op->n[1] * op->n[2], nin, s);
+}
+
 extern "C" int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method, void* func,
                                   const void* source, int nrelax, double w, void* stream) {
   if (!op) return set_error(GFD_EINVAL, "null operator");

@@ -31,7 +31,7 @@ namespace gfd {
 constexpr int kMaxR = 6;      // largest star radius (stencil order 2*6)
 constexpr int kMaxCoefs = 128;  // general kernel
 
-enum { MODE_APPLY = 0, MODE_JACOBI = 1, MODE_RESIDUAL = 2 };
+enum { MODE_APPLY = 0, MODE_JACOBI = 1, MODE_RESIDUAL = 2, MODE_POTENTIAL = 3 };
 
 template <class S>
 struct StarParams {
@@ -48,6 +48,7 @@ struct StarParams {
   int fix_yz;       // complex: the tile needs y/z Bloch phases on wrapped cells
   Phases<S> P;
   double* partials; // MODE_RESIDUAL: one sum of r^2 per CTA (or nullptr)
+  const void* pot;  // MODE_POTENTIAL: real potential v (one grid, type S)
 };
 
 // Asynchronous global->shared copies (sm_80+ cp.async).  A source size of 0
@@ -90,9 +91,12 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
-template <int BZ, int TY, int VY, int R, int S, class V, bool RHO>
+template <int BZ, int TY, int VY, int R, int S, class V, int MODE>
 constexpr size_t star_smem_bytes() {
-  return size_t(S) * ((TY * VY + 2 * R) * (BZ + 2 * R) + (RHO ? TY * VY * BZ : 0)) * sizeof(V);
+  constexpr bool RHO = MODE == MODE_JACOBI || MODE == MODE_RESIDUAL;
+  constexpr bool POT = MODE == MODE_POTENTIAL;
+  return size_t(S) * ((TY * VY + 2 * R) * (BZ + 2 * R) + (RHO ? TY * VY * BZ : 0)) * sizeof(V) +
+         (POT ? size_t(S) * TY * VY * BZ * sizeof(typename vt<V>::S) : 0);
 }
 
 // Axis-aligned ("star") stencil, marching along axis 0.
@@ -125,13 +129,15 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
   constexpr int SY = BY + 2 * R, SZ = BZ + 2 * R, CELLS = SY * SZ;
   constexpr int CPT = (CELLS + NT - 1) / NT;
   constexpr int Q = 2 * R + 1;
-  constexpr bool RHO = MODE != MODE_APPLY;
+  constexpr bool RHO = MODE == MODE_JACOBI || MODE == MODE_RESIDUAL;
+  constexpr bool POT = MODE == MODE_POTENTIAL;
   constexpr int RCELLS = RHO ? BY * BZ : 0;
   static_assert(S >= 2, "pipeline needs two stages");
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* tiles = reinterpret_cast<V*>(smem_raw);  // [S][CELLS]
   V* rtiles = tiles + S * CELLS;              // [S][BY*BZ] source terms
+  Sc* vtiles = reinterpret_cast<Sc*>(rtiles + S * RCELLS);  // [S][BY*BZ] potential
   __shared__ double red[NT / 32 > 0 ? NT / 32 : 1];
 
   const int t = threadIdx.x, tz = t % BZ, ty = t / BZ;
@@ -187,6 +193,8 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
   }
   const unsigned smem0 = smem_addr(tiles);
   const unsigned rsmem0 = smem_addr(rtiles);
+  const unsigned vsmem0 = smem_addr(vtiles);
+  const char* pot_c = reinterpret_cast<const char*>(p.pot);
   const size_t plane_b = size_t(plane) * sizeof(V);
   const char* inb_c = reinterpret_cast<const char*>(inb);
   const char* rho_c = reinterpret_cast<const char*>(rhob);
@@ -231,6 +239,21 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
               asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d),
                            "l"(rsrc + own_b[j]), "n"(int(sizeof(V))), "r"(n)
                            : "memory");
+          }
+        }
+      }
+      if constexpr (POT) {
+        // The potential of this plane's own points (same stage as the plane).
+        if (P >= x0 && P < x1) {
+          const unsigned vbase = vsmem0 + unsigned((st * BY * BZ + ty * VY * BZ + tz) * sizeof(Sc));
+          const char* vsrc = pot_c + size_t(P) * size_t(plane) * sizeof(Sc);
+#pragma unroll
+          for (int j = 0; j < VY; j++) {
+            const unsigned n = own_in[j] ? unsigned(sizeof(Sc)) : 0u;
+            const unsigned d = vbase + unsigned(j * BZ * sizeof(Sc));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d),
+                         "l"(vsrc + own_b[j] / vt<V>::NC), "n"(int(sizeof(Sc))), "r"(n)
+                         : "memory");
           }
         }
       }
@@ -285,7 +308,9 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
           for (int j = 0; j < VY; j++) {
             own[j] = col[R + j];
             const V* row = colp + (R + j) * SZ;
-            V sy = vmul(p.c0, col[R + j]);
+            Sc cc = p.c0;
+            if constexpr (POT) cc += vtiles[st * BY * BZ + ty * VY * BZ + tz + j * BZ];
+            V sy = vmul(cc, col[R + j]);
             V sz = vzero<V>();
 #pragma unroll
             for (int k = 1; k <= R; k++) {
@@ -328,7 +353,7 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
 #pragma unroll
           for (int j = 0; j < VY; j++) {
             V* dst = reinterpret_cast<V*>(dstp + own_b[j]);
-            if constexpr (MODE == MODE_APPLY) {
+            if constexpr (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) {
               if (own_in[j]) stcs(dst, acc[j][qs]);
             } else if constexpr (MODE == MODE_JACOBI) {
               static_assert(vt<V>::NC == 1, "relaxation is real only");
@@ -375,6 +400,7 @@ __global__ void __launch_bounds__(256)
 star_direct_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
                    const StarParams<typename vt<V>::S> p, long long total) {
   pdl_enter();
+  using Sc = typename vt<V>::S;
   __shared__ double red[8];
   const long long plane = (long long)p.n1 * p.n2;
   double sumsq = 0.0;
@@ -385,7 +411,9 @@ star_direct_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __res
     const int r1 = int(rem - i0 * plane);
     const int i1 = r1 / p.n2, i2 = r1 - i1 * p.n2;
     const V* base = in + b * p.band;
-    V s = vmul(p.c0, ldro(in + g));
+    Sc cc = p.c0;
+    if constexpr (MODE == MODE_POTENTIAL) cc += ldro(static_cast<const Sc*>(p.pot) + rem);
+    V s = vmul(cc, ldro(in + g));
 #pragma unroll
     for (int k = -R; k <= R; k++) {
       if (k == 0) continue;
@@ -409,7 +437,7 @@ star_direct_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __res
         madd(s, p.cz[kMaxR + k], v);
       }
     }
-    if constexpr (MODE == MODE_APPLY) {
+    if constexpr (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) {
       out[g] = s;
     } else if constexpr (MODE == MODE_JACOBI) {
       static_assert(vt<V>::NC == 1, "relaxation is real only");

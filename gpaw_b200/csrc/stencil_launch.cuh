@@ -69,7 +69,7 @@ inline LaunchGeom star_geom(const gfd_operator* op, int tile, int64_t nin, int R
   int gx = (op->n[2] + td.BZ - 1) / td.BZ;
   int gy = (op->n[1] + td.BY - 1) / td.BY;
   int64_t tiles = (int64_t)gx * gy * std::max<int64_t>(nin, 1);
-  int64_t target = 4LL * num_sms();
+  int64_t target = (int64_t)march_ctas_per_sm() * num_sms();
   int maxc = std::max(1, op->n[0] / std::max(4, 2 * R));
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   g.x_chunk = (op->n[0] + nxc - 1) / nxc;
@@ -93,7 +93,7 @@ int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t n
             const StarParams<typename vt<V>::S>& base, const LaunchGeom& g, double* partials,
             cudaStream_t s) {
   constexpr int S = kStages;
-  constexpr size_t smem = star_smem_bytes<BZ, TY, VY, R, S, V, MODE != MODE_APPLY>();
+  constexpr size_t smem = star_smem_bytes<BZ, TY, VY, R, S, V, MODE>();
   auto kern = star_kernel<V, R, BZ, TY, VY, S, MODE>;
   int st = raise_smem_limit(kern, smem, "cudaFuncSetAttribute(star_kernel)");
   if (st) return st;
@@ -253,11 +253,15 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
   V* vout = static_cast<V*>(out);
   const V* vrho = static_cast<const V*>(rho);
   if constexpr (vt<V>::NC == 2) {
-    if (mode != OP_APPLY) return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
+    if (mode != OP_APPLY && mode != OP_POTENTIAL)
+      return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
   }
+  if (mode == OP_POTENTIAL) p.pot = rho;  // the potential travels as the source argument
   if (use_direct(op, nin)) {
     p.partials = partials;
     const long long total = (long long)p.band * nin;
+    if (mode == OP_POTENTIAL)
+      return direct_dispatch<V, MODE_POTENTIAL>(op, vin, vout, nullptr, p, total, s);
     if constexpr (vt<V>::NC == 1) {
       if (mode == OP_JACOBI) return direct_dispatch<V, MODE_JACOBI>(op, vin, vout, vrho, p, total, s);
       if (mode == OP_RESIDUAL)
@@ -277,6 +281,8 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
   LaunchGeom g = star_geom(op, tile, nin, op->R);
   p.nxc = g.nxc;
   p.x_chunk = g.x_chunk;
+  if (mode == OP_POTENTIAL)
+    return star_dispatch<V, MODE_POTENTIAL>(op, tile, vin, vout, nullptr, nin, p, g, nullptr, s);
   if constexpr (vt<V>::NC == 1) {
     if (mode == OP_JACOBI)
       return star_dispatch<V, MODE_JACOBI>(op, tile, vin, vout, vrho, nin, p, g, nullptr, s);

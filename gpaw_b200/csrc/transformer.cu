@@ -28,7 +28,7 @@ static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t n
   const size_t smem = (size_t)(2 * RY * RZ + 2 * RY * BZC) * sizeof(V);
   const int gx = (tr->nout[2] + BZC - 1) / BZC, gy = (tr->nout[1] + BYC - 1) / BYC;
   const int64_t tiles = (int64_t)gx * gy * nin;
-  const int64_t target = 4LL * num_sms();
+  const int64_t target = (int64_t)march_ctas_per_sm() * num_sms();
   int maxc = std::max(1, tr->nout[0] / 2);
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   p.x_chunk = (tr->nout[0] + nxc - 1) / nxc;
@@ -53,7 +53,7 @@ static int interp_go(const gfd_transformer* tr, const V* in, V* out, const V* ba
   const size_t smem = (size_t)(2 * CY * CZ + 2 * CY * BZF) * sizeof(V);
   const int gx = (tr->nout[2] + BZF - 1) / BZF, gy = (tr->nout[1] + BYF - 1) / BYF;
   const int64_t tiles = (int64_t)gx * gy * nin;
-  const int64_t target = 4LL * num_sms();
+  const int64_t target = (int64_t)march_ctas_per_sm() * num_sms();
   int maxc = std::max(1, tr->nout[0] / 4);
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   p.x_chunk = (tr->nout[0] + nxc - 1) / nxc;

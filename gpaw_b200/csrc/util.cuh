@@ -55,6 +55,21 @@ __global__ void __launch_bounds__(256) convert_kernel(Y* __restrict__ y, const X
   }
 }
 
+// out[b][i] += v[i] * in[b][i] for nb bands of n points (v real).
+template <class V>
+__global__ void __launch_bounds__(256) add_potential_kernel(V* __restrict__ out,
+                                                            const V* __restrict__ in,
+                                                            const typename vt<V>::S* __restrict__ v,
+                                                            long long n, long long total) {
+  pdl_enter();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    V o = out[i];
+    madd(o, v[i % n], in[i]);
+    out[i] = o;
+  }
+}
+
 // Per-block partial sums of a[i] (SQUARE: a[i]^2), in a fixed order.
 template <class T, bool SQUARE>
 __global__ void __launch_bounds__(kRedThreads) partial_sum_kernel(const T* __restrict__ a,

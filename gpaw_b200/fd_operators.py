@@ -17,6 +17,7 @@ from fractions import Fraction
 from math import factorial
 
 import numpy as np
+import torch
 
 from . import _lib
 from .tensors import dtype_code, is_complex, nbands, require_device, stream_of, torch_dtype
@@ -111,6 +112,24 @@ class FDOperator:
         _lib.check(_lib.lib.gfd_operator_apply(
             self.operator, dtype_code(in_xg), in_xg.data_ptr(), out_xg.data_ptr(),
             nbands(in_xg), pp, stream_of(in_xg)), 'apply')
+
+    def apply_with_potential(self, in_xg, out_xg, vt_g, phase_cd=None):
+        """out_xg = operator(in_xg) + vt_g * in_xg in one pass: the kinetic
+        operator and the local potential of FDWaveFunctions.
+        apply_pseudo_hamiltonian (gpaw/wavefunctions/fd.py:50-52 with
+        gpaw/hamiltonian.py:371-398).  vt_g: one real grid on the device,
+        float64 for float64/complex128 bands, float32 for float32/complex64."""
+        self._check_arrays(in_xg, out_xg)
+        require_device(vt_g, 'vt_g')
+        if tuple(vt_g.shape) != self.shape:
+            raise ValueError('vt_g must have the grid shape %s' % (self.shape,))
+        want = torch.float32 if in_xg.dtype in (torch.float32, torch.complex64) else torch.float64
+        if vt_g.dtype != want or not vt_g.is_contiguous():
+            raise ValueError('vt_g must be a contiguous %s grid' % want)
+        _, pp = _lib.phases_arg(phase_cd if is_complex(in_xg.dtype) else None)
+        _lib.check(_lib.lib.gfd_operator_apply_potential(
+            self.operator, dtype_code(in_xg), in_xg.data_ptr(), out_xg.data_ptr(),
+            nbands(in_xg), pp, vt_g.data_ptr(), stream_of(in_xg)), 'apply_with_potential')
 
     def relax(self, relax_method, f_g, s_g, n, w=None):
         """n relaxation sweeps for 'operator f_g = s_g', in place on f_g.

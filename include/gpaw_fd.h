@@ -133,6 +133,19 @@ GFD_API int gfd_operator_relax_noalloc(gfd_operator* op, int dtype, int relax_me
  * c/operators.c:408-421). */
 GFD_API int gfd_operator_get_diagonal_element(const gfd_operator* op, double* d);
 
+/* out = L in + v * in for nin bands: the kinetic operator and the local
+ * potential in one pass.  Replaces FDWaveFunctions.apply_pseudo_hamiltonian
+ * (gpaw/wavefunctions/fd.py:50-52): kin.apply(psit, Htpsit, phase_cd)
+ * followed by Hamiltonian.apply_local_potential (gpaw/hamiltonian.py:
+ * 371-398, Htpsit += psit * vt).  v: device grid of n0*n1*n2 real values,
+ * float64 for float64/complex128 bands and float32 for float32/complex64.
+ * Axis-aligned operators fuse the potential into the stencil's centre
+ * weight (one read and one write per band); other offset sets add it in a
+ * second pass. */
+GFD_API int gfd_operator_apply_potential(gfd_operator* op, int dtype, const void* in, void* out,
+                                         int64_t nin, const double* phase_cd, const void* v,
+                                         void* stream);
+
 /* Device-side error flags of the current device, then cleared: *flags != 0
  * when a stencil kernel gave up on a bounded wait since the last call (its
  * output is then incomplete).  No counterpart in the reference, whose CPU

@@ -288,3 +288,51 @@ def test_tma_fed_kernel_in_subprocess(cuda):
                        cwd=root, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
     assert ' passed' in r.stdout
+
+
+@pytest.mark.parametrize('case', ['bloch96', 'plain48', 'small', 'hex'])
+def test_pseudo_hamiltonian_fused(cuda, case):
+    """kin psit + vt psit in one pass against the oracle stencil plus the
+    reference's numpy update Htpsit += psit * vt (gpaw/hamiltonian.py:
+    395-398): complex128 Bloch bands on 96^3 (marching kernel), float64 on
+    47^3 zero boundary, a small grid (one-thread-per-point kernel) and a
+    hexagonal cell (cross terms: stencil, then the potential pass)."""
+    import torch
+    from gpaw_b200.fd_operators import FDOperator
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.hamiltonian import apply_pseudo_hamiltonian
+    rng = np.random.default_rng(31)
+    if case == 'bloch96':
+        gd = G.Grid((96,) * 3, (96 * 0.18 / BOHR,) * 3, 1)
+        shape = (2,) + tuple(gd.n_c)
+        a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        ph = G.bloch_phases(gd, (0.25, 0.0, 0.0))
+    elif case == 'plain48':
+        gd = G.Grid((48,) * 3, (48 * 0.2 / BOHR,) * 3, 0)
+        a = rng.uniform(-1, 1, (3,) + tuple(gd.n_c))
+        ph = None
+    elif case == 'small':
+        gd = G.Grid((12, 10, 14), (3.6, 3.0, 4.2), (1, 0, 1))
+        a = rng.standard_normal((2,) + tuple(gd.n_c)) + 1j * rng.standard_normal((2,) + tuple(gd.n_c))
+        ph = G.bloch_phases(gd, (0.1, 0.0, -0.3))
+    else:
+        gd = G.Grid((8, 8, 8), np.array([(1, 0, 0), (0.5, 3 ** 0.5 / 2, 0), (0, 0, 1.1)]) * 4.0, 1)
+        a = rng.standard_normal((2,) + tuple(gd.n_c)) + 1j * rng.standard_normal((2,) + tuple(gd.n_c))
+        ph = G.bloch_phases(gd, (0.1, -0.2, 0.3))
+    c, o = G.laplace_stencil(gd, -0.5, 3 if case != 'hex' else 2)
+    vt = rng.uniform(-2, 1, tuple(gd.n_c))
+    ref = K.fd_apply(c, o, gd.pbc_c, a, ph, nthreads=8) + a * vt
+    gdp = GridDescriptor(gd.N_c, gd.cell_cv, gd.pbc_c)
+    t = dev(a, cuda)
+    kin = FDOperator(c, o, gdp, t.dtype)
+    out = torch.empty_like(t)
+    apply_pseudo_hamiltonian(kin, t, out, dev(vt, cuda), ph)
+    assert rel_err(host(out), ref) < TOL
+    # FP32 variant against the FP64 oracle
+    t32 = t.to(torch.complex64 if t.is_complex() else torch.float32)
+    kin32 = FDOperator(c, o, gdp, t32.dtype)
+    o32 = torch.empty_like(t32)
+    kin32.apply_with_potential(t32, o32, dev(vt, cuda).float(), ph)
+    assert rel_err(host(o32).astype(ref.dtype), ref) < 2e-6
+    with pytest.raises(ValueError):
+        kin.apply_with_potential(t, out, dev(vt, cuda).float(), ph)  # wrong potential dtype
