@@ -429,6 +429,78 @@ def hamiltonian_bench(lap, a, b, phase, steps):
 
 
 # ---------------------------------------------------------------------------
+# Band preconditioner (gpaw/preconditioner.py) on the headline bands: the
+# eight-pass device form against the reference's nineteen-operation
+# sequence written with this library's unfused calls.
+# ---------------------------------------------------------------------------
+def preconditioner_bench(gd, lap, a, b, phase, steps):
+    import torch
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.preconditioner import Preconditioner
+    from gpaw_b200.transformers import Transformer
+    nb = a.shape[0]
+    pc = Preconditioner(gd, lap, complex, block=nb)
+    gd1 = gd.coarsen()
+    gd2 = gd1.coarsen()
+    kin1 = Laplace(gd1, -0.5, 1, complex)
+    kin2 = Laplace(gd2, -0.5, 1, complex)
+    r0, r1_ = Transformer(gd, gd1, 1, complex), Transformer(gd1, gd2, 1, complex)
+    i2, i1 = Transformer(gd2, gd1, 1, complex), Transformer(gd1, gd, 1, complex)
+    sh1 = (nb,) + tuple(int(x) for x in gd1.n_c)
+    sh2 = (nb,) + tuple(int(x) for x in gd2.n_c)
+    r1, d1, q1 = (torch.empty(sh1, dtype=a.dtype, device=a.device) for _ in range(3))
+    r2, q2 = (torch.empty(sh2, dtype=a.dtype, device=a.device) for _ in range(2))
+    step = pc.step
+
+    class K:
+        phase_cd = phase
+
+    def unfused():
+        # gpaw/preconditioner.py:48-70, one array operation per line
+        r0.apply(-a, r1, phase)
+        d1.copy_(4 * step * r1)
+        kin1.apply(d1, q1, phase)
+        q1.sub_(r1)
+        r1_.apply(q1, r2, phase)
+        d2 = 16 * step * r2
+        kin2.apply(d2, q2, phase)
+        q2.sub_(r2)
+        d2.sub_(16 * step * q2)
+        i2.apply(d2, q1, phase)
+        d1.sub_(q1)
+        kin1.apply(d1, q1, phase)
+        q1.sub_(r1)
+        d1.sub_(4 * step * q1)
+        i1.apply(-d1, b, phase)
+        q0 = torch.empty_like(b)
+        lap.apply(b, q0, phase)
+        q0.sub_(a)
+        b.add_(q0, alpha=-step)
+        b.mul_(-1.0)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    fused_ms = timed(lambda: pc(a, K))
+    unfused_ms = timed(unfused)
+    del pc
+    return {'workload': 'Preconditioner (gpaw/preconditioner.py), %d complex128 bands x %d^3, '
+                        'kin0 nn=3, k=(0.25,0,0)' % (nb, a.shape[1]),
+            'device_passes_ms': fused_ms, 'reference_sequence_ms': unfused_ms,
+            'speedup': unfused_ms / fused_ms}
+
+
+# ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args):
@@ -495,9 +567,10 @@ def run_gpu_arm(args):
                'd2h_bytes_per_step': nbytes // 2}
         del host_in, host_out
 
-    ham = None
+    ham = pcb = None
     if rank == 0 and world == 1 and not args.no_hamiltonian:
         ham = hamiltonian_bench(lap, a, b, phase, min(args.steps, 20))
+        pcb = preconditioner_bench(gd, lap, a, b, phase, min(args.steps, 10))
 
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic()
@@ -515,6 +588,8 @@ def run_gpu_arm(args):
             'clocks': clocks.result()}
     if ham is not None:
         line['hamiltonian'] = ham
+    if pcb is not None:
+        line['preconditioner'] = pcb
     if rank == 0 and world == 1 and not args.no_poisson:
         try:
             pb, _, _, _ = poisson_bench()

@@ -51,6 +51,11 @@ SIGNATURES = {
                                                   ctypes.c_int, ctypes.c_double, _vp]),
     'gfd_operator_get_diagonal_element': (ctypes.c_int, [_vp, _dp]),
     'gfd_device_errors': (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    'gfd_preconditioner_create': (ctypes.c_int, [_vp] * 7 + [ctypes.c_int, ctypes.c_int64,
+                                                             ctypes.POINTER(_vp)]),
+    'gfd_preconditioner_destroy': (ctypes.c_int, [_vp]),
+    'gfd_preconditioner_apply': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int64, _dp,
+                                                _vp]),
     'gfd_operator_apply_potential': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int64, _dp, _vp, _vp]),
     'gfd_transformer_create': (ctypes.c_int, [_i64p, _i64p, ctypes.c_int, _i64p, _i64p, _i64p,
                                               _i64p, ctypes.c_int, ctypes.c_int,

@@ -43,13 +43,15 @@ struct gfd_transformer {
 
 namespace gfd {
 
-enum { OP_APPLY = 0, OP_JACOBI = 1, OP_RESIDUAL = 2, OP_POTENTIAL = 3 };
+enum { OP_APPLY = 0, OP_JACOBI = 1, OP_RESIDUAL = 2, OP_POTENTIAL = 3, OP_JACOBI_NEG = 4 };
 
 int num_sms();
 
 // Stencil launch.  mode OP_APPLY: out = L in.  OP_JACOBI: out = Jacobi update
 // of in with source rho and weight w.  OP_RESIDUAL: out = L in - rho and, if
 // partials != nullptr, one sum of squares per CTA into partials.
+// OP_JACOBI_NEG: minus the Jacobi update (exact sign flip).  Complex dtypes
+// support the Jacobi / residual modes for radius <= 3.
 // OP_POTENTIAL (star operators only): out = L in + v in with the real grid v
 // (float64 for float64/complex128 bands, float32 otherwise) passed as rho.
 // in/out/rho point to nin bands.  phase_cd: 12 doubles (host) or nullptr.
@@ -70,6 +72,12 @@ int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, i
 // (the first weighted-Jacobi sweep of the coarse level from a zero guess).
 int tr_launch_seed(const gfd_transformer* tr, int dtype, const void* in, void* out, void* seed,
                    double seed_scale, cudaStream_t s);
+// General form: out = out_scale * transfer(in) (interpolation with base:
+// out = base - out_scale * interpolate(in)); restriction with seed also
+// writes seed = seed_scale * out.  out_scale must be 1 or -1 (exact).
+int tr_launch_ex(const gfd_transformer* tr, int dtype, const void* in, void* out,
+                 const void* base, int64_t nin, const double* phases, double out_scale,
+                 void* seed, double seed_scale, cudaStream_t s);
 // Interpolation with the correction fused: out = base - interpolate(in)
 // (in place when base == out).
 int tr_launch_sub(const gfd_transformer* tr, int dtype, const void* in, void* out,

@@ -44,7 +44,7 @@ struct StarParams {
   S cx[2 * kMaxR + 1];  // weight of offset k along axis 0 at index kMaxR + k
   S cy[2 * kMaxR + 1];
   S cz[2 * kMaxR + 1];
-  S wc;             // MODE_JACOBI: w / coefs[0]
+  S wc;             // MODE_JACOBI: w / coefs[0] (negated for the negated sweep)
   int fix_yz;       // complex: the tile needs y/z Bloch phases on wrapped cells
   Phases<S> P;
   double* partials; // MODE_RESIDUAL: one sum of r^2 per CTA (or nullptr)
@@ -356,8 +356,7 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
             if constexpr (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) {
               if (own_in[j]) stcs(dst, acc[j][qs]);
             } else if constexpr (MODE == MODE_JACOBI) {
-              static_assert(vt<V>::NC == 1, "relaxation is real only");
-              if (own_in[j]) stcs(dst, p.wc * (rt[j * BZ] - acc[j][qs]));
+              if (own_in[j]) stcs(dst, vmul(p.wc, vsub(rt[j * BZ], acc[j][qs])));
             } else {
               const V r = vsub(acc[j][qs], rt[j * BZ]);
               if (own_in[j]) {
@@ -440,8 +439,7 @@ star_direct_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __res
     if constexpr (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) {
       out[g] = s;
     } else if constexpr (MODE == MODE_JACOBI) {
-      static_assert(vt<V>::NC == 1, "relaxation is real only");
-      out[g] = p.wc * (ldro(rho + g) - s);
+      out[g] = vmul(p.wc, vsub(ldro(rho + g), s));
     } else {
       const V r = vsub(s, ldro(rho + g));
       out[g] = r;
@@ -469,6 +467,7 @@ struct GenParams {
   S coefs[kMaxCoefs];
   signed char off[kMaxCoefs][3];
   S w;
+  S sign;           // MODE_JACOBI: +1, or -1 for the negated sweep (exact)
   Phases<S> P;
   double* partials;
 };
@@ -536,10 +535,15 @@ general_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restric
           V src = ldro(rhob + q * plane + (long long)y * p.n2 + z);
           if constexpr (MODE == MODE_JACOBI) {
             // coefs[0] is the diagonal (c/bmgs/relax.c:46-71)
-            static_assert(vt<V>::NC == 1, "relaxation is real only");
             const V* sl = ring + ((q - (x0 - mp)) % NR) * CELLS;
             V ctr = sl[(mp + ty + j * TY) * SZ + (mp + tz)];
-            *dst = (S(1) - p.w) * ctr + p.w * (src - s) / p.coefs[0];
+            if constexpr (vt<V>::NC == 1) {
+              *dst = p.sign * ((S(1) - p.w) * ctr + p.w * (src - s) / p.coefs[0]);
+            } else {
+              const V d = vsub(src, s);
+              *dst = {p.sign * ((S(1) - p.w) * ctr.re + p.w * d.re / p.coefs[0]),
+                      p.sign * ((S(1) - p.w) * ctr.im + p.w * d.im / p.coefs[0])};
+            }
           } else {
             V r = vsub(s, src);
             *dst = r;

@@ -112,6 +112,10 @@ int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t n
 // Wide tile: 32 columns x 16 rows; 4 rows per thread for 8-byte and
 // smaller values, 2 rows per thread where 4 would exceed the register file
 // (16-byte values or radius > 3).
+// Complex Jacobi / residual sweeps (the band preconditioner) are built for
+// radii up to 3 only, which keeps the number of kernels in check.
+constexpr int kMaxComplexRelaxR = 3;
+
 template <class V, int R, int MODE>
 int star_wide(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
               const StarParams<typename vt<V>::S>& p, const LaunchGeom& g, double* partials,
@@ -133,9 +137,13 @@ int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V
     if (tile == TILE_MID)                                                                    \
       return star_go<V, RR, 16, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);       \
     return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
-#define GFD_STAR_WIDE(RR) \
-  case RR:                \
-    return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
+#define GFD_STAR_WIDE(RR)                                                                    \
+  case RR:                                                                                   \
+    if constexpr (RR > kMaxComplexRelaxR && vt<V>::NC == 2 && MODE != MODE_APPLY &&          \
+                  MODE != MODE_POTENTIAL)                                                    \
+      return set_error(GFD_EUNSUPPORTED, "complex Jacobi/residual sweeps need radius <= 3"); \
+    else                                                                                     \
+      return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
   switch (op->R) {
     GFD_STAR_SMALL(1)
     GFD_STAR_SMALL(2)
@@ -210,6 +218,15 @@ template <class V, int MODE>
 int direct_dispatch(const gfd_operator* op, const V* in, V* out, const V* rho,
                     const StarParams<typename vt<V>::S>& p, long long total, cudaStream_t s) {
   const int blocks = direct_blocks(total);
+  if constexpr (vt<V>::NC == 2 && MODE != MODE_APPLY && MODE != MODE_POTENTIAL) {
+    switch (op->R) {
+      case 1: launch_k(star_direct_kernel<V, 1, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+      case 2: launch_k(star_direct_kernel<V, 2, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+      case 3: launch_k(star_direct_kernel<V, 3, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
+      default: return set_error(GFD_EUNSUPPORTED, "complex Jacobi/residual sweeps need radius <= 3");
+    }
+    return check_launch("star_direct_kernel");
+  }
   switch (op->R) {
     case 1: launch_k(star_direct_kernel<V, 1, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
     case 2: launch_k(star_direct_kernel<V, 2, MODE>, blocks, 256, 0, s, in, out, rho, p, total); break;
@@ -237,10 +254,12 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
     p.cy[i] = S(op->cy[i]);
     p.cz[i] = S(op->cz[i]);
   }
-  if (mode == OP_JACOBI) {
-    // Fold (1 - w) phi into the centre weight (see star_kernel).
+  if (mode == OP_JACOBI || mode == OP_JACOBI_NEG) {
+    // Fold (1 - w) phi into the centre weight (see star_kernel); the
+    // negated sweep flips the sign of w / c0, which is exact.
     p.c0 = S(-(1.0 - w) * op->c0 / w);
     p.wc = S(w / op->c0);
+    if (mode == OP_JACOBI_NEG) p.wc = -p.wc;
   }
   fill_phases(p.P, phase_cd);
   p.fix_yz = 0;
@@ -252,9 +271,10 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
   const V* vrho = static_cast<const V*>(rho);
+  const bool relax_mode = mode == OP_JACOBI || mode == OP_JACOBI_NEG || mode == OP_RESIDUAL;
   if constexpr (vt<V>::NC == 2) {
-    if (mode != OP_APPLY && mode != OP_POTENTIAL)
-      return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
+    if (relax_mode && op->R > kMaxComplexRelaxR)
+      return set_error(GFD_EUNSUPPORTED, "complex Jacobi/residual sweeps need radius <= 3");
   }
   if (mode == OP_POTENTIAL) p.pot = rho;  // the potential travels as the source argument
   if (use_direct(op, nin)) {
@@ -262,11 +282,10 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
     const long long total = (long long)p.band * nin;
     if (mode == OP_POTENTIAL)
       return direct_dispatch<V, MODE_POTENTIAL>(op, vin, vout, nullptr, p, total, s);
-    if constexpr (vt<V>::NC == 1) {
-      if (mode == OP_JACOBI) return direct_dispatch<V, MODE_JACOBI>(op, vin, vout, vrho, p, total, s);
-      if (mode == OP_RESIDUAL)
-        return direct_dispatch<V, MODE_RESIDUAL>(op, vin, vout, vrho, p, total, s);
-    }
+    if (mode == OP_JACOBI || mode == OP_JACOBI_NEG)
+      return direct_dispatch<V, MODE_JACOBI>(op, vin, vout, vrho, p, total, s);
+    if (mode == OP_RESIDUAL)
+      return direct_dispatch<V, MODE_RESIDUAL>(op, vin, vout, vrho, p, total, s);
     return direct_dispatch<V, MODE_APPLY>(op, vin, vout, nullptr, p, total, s);
   }
   if constexpr (std::is_same_v<V, cplx<double>>) {
@@ -283,12 +302,10 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
   p.x_chunk = g.x_chunk;
   if (mode == OP_POTENTIAL)
     return star_dispatch<V, MODE_POTENTIAL>(op, tile, vin, vout, nullptr, nin, p, g, nullptr, s);
-  if constexpr (vt<V>::NC == 1) {
-    if (mode == OP_JACOBI)
-      return star_dispatch<V, MODE_JACOBI>(op, tile, vin, vout, vrho, nin, p, g, nullptr, s);
-    if (mode == OP_RESIDUAL)
-      return star_dispatch<V, MODE_RESIDUAL>(op, tile, vin, vout, vrho, nin, p, g, partials, s);
-  }
+  if (mode == OP_JACOBI || mode == OP_JACOBI_NEG)
+    return star_dispatch<V, MODE_JACOBI>(op, tile, vin, vout, vrho, nin, p, g, nullptr, s);
+  if (mode == OP_RESIDUAL)
+    return star_dispatch<V, MODE_RESIDUAL>(op, tile, vin, vout, vrho, nin, p, g, partials, s);
   return star_dispatch<V, MODE_APPLY>(op, tile, vin, vout, nullptr, nin, p, g, nullptr, s);
 }
 
@@ -336,17 +353,16 @@ int launch_general_typed(const gfd_operator* op, int mode, const void* in, void*
     for (int a = 0; a < 3; a++) p.off[c][a] = (signed char)op->off[3 * c + a];
   }
   p.w = S(w);
+  p.sign = mode == OP_JACOBI_NEG ? S(-1) : S(1);
   fill_phases(p.P, phase_cd);
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
   const V* vrho = static_cast<const V*>(rho);
-  if constexpr (vt<V>::NC == 1) {
-    if (mode == OP_JACOBI) return general_go<V, MODE_JACOBI>(op, vin, vout, vrho, nin, p, nullptr, s);
-    if (mode == OP_RESIDUAL)
-      return general_go<V, MODE_RESIDUAL>(op, vin, vout, vrho, nin, p, partials, s);
-  } else {
-    if (mode != OP_APPLY) return set_error(GFD_EINVAL, "relaxation/residual need a real dtype");
-  }
+  if (mode == OP_JACOBI || mode == OP_JACOBI_NEG)
+    return general_go<V, MODE_JACOBI>(op, vin, vout, vrho, nin, p, nullptr, s);
+  if (mode == OP_RESIDUAL)
+    return general_go<V, MODE_RESIDUAL>(op, vin, vout, vrho, nin, p, partials, s);
+  if (mode != OP_APPLY) return set_error(GFD_EUNSUPPORTED, "mode not available for this stencil");
   return general_go<V, MODE_APPLY>(op, vin, vout, nullptr, nin, p, nullptr, s);
 }
 

@@ -71,6 +71,9 @@ struct TrParams {
   // out of the restriction that produces its rho.
   void* seed;
   S seed_scale;
+  // Factor on the transferred value (1, or -1 for the negated transfers of
+  // the band preconditioner; multiplying by -1 is exact).
+  S out_scale;
 };
 
 // Pack an in-plane source offset and its wrap sides; -1 = zero point.
@@ -196,6 +199,7 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
           const int y = Y0 + ty + j * TYC, z = Z0 + tz;
           if (y < p.no1 && z < p.no2) {
             V v = rst_tap<NN, V>([&](int o) { return q[j][W + o]; });
+            if (p.out_scale != S(1)) v = vmul(p.out_scale, v);
             const long long o = X * plane_out + (long long)y * p.no2 + z;
             stcs(outb + o, v);
             if (p.seed) stcs(static_cast<V*>(p.seed) + (outb - out) + o, vmul(p.seed_scale, v));
@@ -322,6 +326,7 @@ interp_kernel(const V* __restrict__ in, V* out, const V* base,
           if (y < p.no1 && z < p.no2) {
             V v = par ? ip_tap<NN, V>([&](int o) { return q[j][NN - 1 + o]; }) : q[j][NN - 1];
             const long long o = X * plane_out + (long long)y * p.no2 + z;
+            if (p.out_scale != S(1)) v = vmul(p.out_scale, v);
             if constexpr (SUB) v = vsub(baseb[o], v);
             stcs(outb + o, v);
           }
@@ -370,11 +375,12 @@ restrict_direct_kernel(const V* __restrict__ in, V* __restrict__ out,
     const V* base = in + b * p.band_in;
     // fine centre of each axis: 2i + (2nn-1) - lo
     const int fx = 2 * X + W - p.lo0, fy = 2 * Y + W - p.lo1, fz = 2 * Z + W - p.lo2;
-    const V v = rst_tap<NN, V>([&](int ox) {
+    V v = rst_tap<NN, V>([&](int ox) {
       return rst_tap<NN, V>([&](int oy) {
         return rst_tap<NN, V>([&](int oz) { return tr_fetch(base, fx + ox, fy + oy, fz + oz, p); });
       });
     });
+    if (p.out_scale != typename vt<V>::S(1)) v = vmul(p.out_scale, v);
     out[g] = v;
     if (p.seed) static_cast<V*>(p.seed)[g] = vmul(p.seed_scale, v);
   }
@@ -403,6 +409,7 @@ interp_direct_kernel(const V* __restrict__ in, V* out, const V* base_out,
         return along(gz & 1, [&](int oz) { return tr_fetch(base, cx + ox, cy + oy, cz + oz, p); });
       });
     });
+    if (p.out_scale != typename vt<V>::S(1)) v = vmul(p.out_scale, v);
     if constexpr (SUB) v = vsub(base_out[g], v);
     out[g] = v;
   }

@@ -92,7 +92,7 @@ static int direct_go(const gfd_transformer* tr, const V* in, V* out, const V* ba
 template <class V>
 static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const void* base_v,
                     int64_t nin, const double* ph, cudaStream_t s, void* seed = nullptr,
-                    double seed_scale = 0.0) {
+                    double seed_scale = 0.0, double out_scale = 1.0) {
   using S = typename vt<V>::S;
   TrParams<S> p{};
   p.ni0 = tr->nin[0]; p.ni1 = tr->nin[1]; p.ni2 = tr->nin[2];
@@ -105,6 +105,7 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const 
   fill_tr_phases(p.P, ph);
   p.seed = seed;
   p.seed_scale = S(seed_scale);
+  p.out_scale = S(out_scale);
   if (seed && tr->interpolate) return set_error(GFD_EINVAL, "seeded form is for restriction only");
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
@@ -152,11 +153,26 @@ int tr_launch_sub(const gfd_transformer* tr, int dtype, const void* in, void* ou
 
 int tr_launch_seed(const gfd_transformer* tr, int dtype, const void* in, void* out, void* seed,
                    double seed_scale, cudaStream_t s) {
+  return tr_launch_ex(tr, dtype, in, out, nullptr, 1, nullptr, 1.0, seed, seed_scale, s);
+}
+
+int tr_launch_ex(const gfd_transformer* tr, int dtype, const void* in, void* out,
+                 const void* base, int64_t nin, const double* phases, double out_scale,
+                 void* seed, double seed_scale, cudaStream_t s) {
+  if (nin <= 0) return GFD_OK;
   switch (dtype) {
-    case GFD_FLOAT64: return tr_typed<double>(tr, in, out, nullptr, 1, nullptr, s, seed, seed_scale);
-    case GFD_FLOAT32: return tr_typed<float>(tr, in, out, nullptr, 1, nullptr, s, seed, seed_scale);
+    case GFD_FLOAT64:
+      return tr_typed<double>(tr, in, out, base, nin, phases, s, seed, seed_scale, out_scale);
+    case GFD_FLOAT32:
+      return tr_typed<float>(tr, in, out, base, nin, phases, s, seed, seed_scale, out_scale);
+    case GFD_COMPLEX128:
+      return tr_typed<cplx<double>>(tr, in, out, base, nin, phases, s, seed, seed_scale,
+                                    out_scale);
+    case GFD_COMPLEX64:
+      return tr_typed<cplx<float>>(tr, in, out, base, nin, phases, s, seed, seed_scale,
+                                   out_scale);
   }
-  return set_error(GFD_EINVAL, "seeded restriction needs a real dtype");
+  return set_error(GFD_EINVAL, "unknown dtype");
 }
 
 int tr_launch(const gfd_transformer* tr, int dtype, const void* in, void* out, int64_t nin,

@@ -146,6 +146,28 @@ GFD_API int gfd_operator_apply_potential(gfd_operator* op, int dtype, const void
                                          int64_t nin, const double* phase_cd, const void* v,
                                          void* stream);
 
+/* ------------------------------------------------------------------------
+ * Band preconditioner.  Replaces gpaw.preconditioner.Preconditioner
+ * (gpaw/preconditioner.py:13-70): two coarser levels with nn = 1 kinetic
+ * operators (Laplace(gd, -0.5, 1)) and nn = 1 transformers, step =
+ * 0.66666666 / kin0.get_diagonal_element().  The handles are borrowed and
+ * must outlive the preconditioner; block is the most bands per pass (the
+ * scratch holds that many bands on the coarse levels and on the fine grid).
+ * ---------------------------------------------------------------------- */
+typedef struct gfd_preconditioner gfd_preconditioner;
+
+GFD_API int gfd_preconditioner_create(gfd_operator* kin0, gfd_operator* kin1, gfd_operator* kin2,
+                                      gfd_transformer* restrict0, gfd_transformer* restrict1,
+                                      gfd_transformer* interpolate2,
+                                      gfd_transformer* interpolate1, int dtype, int64_t block,
+                                      gfd_preconditioner** out);
+GFD_API int gfd_preconditioner_destroy(gfd_preconditioner* pc);
+/* out = the preconditioned residuals (Preconditioner.__call__,
+ * gpaw/preconditioner.py:45-70) for nb bands; phase_cd: the k-point's Bloch
+ * phases (12 doubles, host) for complex bands, else NULL. */
+GFD_API int gfd_preconditioner_apply(gfd_preconditioner* pc, int dtype, const void* residuals,
+                                     void* out, int64_t nb, const double* phase_cd, void* stream);
+
 /* Device-side error flags of the current device, then cleared: *flags != 0
  * when a stencil kernel gave up on a bounded wait since the last call (its
  * output is then incomplete).  No counterpart in the reference, whose CPU

@@ -182,3 +182,22 @@ def test_port_equals_reference_library():
         ph = G.bloch_phases(gd, (0.3, -0.1, 0.2))
         assert rel_err(K.fd_apply(c, o, gd.pbc_c, ac, ph),
                        K.fd_apply(c, o, gd.pbc_c, ac, ph, impl='ref')) < 1e-15
+
+
+def test_oracle_preconditioner_is_linear():
+    """The restated preconditioner (gpaw/preconditioner.py:45-70) is a linear
+    map of the residuals: P(a R1 + b R2) = a P(R1) + b P(R2), periodic with
+    Bloch phases and zero boundary."""
+    from oracle.preconditioner import Preconditioner as OraclePC
+    rng = np.random.default_rng(12)
+    for N, pbc, k in (((16, 16, 16), 1, (0.25, 0.0, 0.1)), ((16, 12, 20), 0, None)):
+        gd = G.Grid(N, np.array(N) * 0.4, pbc)
+        c, o = G.laplace_stencil(gd, -0.5, 2)
+        pc = OraclePC(gd, (c, o))
+        shape = (2,) + tuple(gd.n_c)
+        R1 = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        R2 = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        ph = G.bloch_phases(gd, k) if k else np.ones((3, 2), complex)
+        lhs = pc(2.0 * R1 - 0.5 * R2, ph)
+        rhs = 2.0 * pc(R1, ph) - 0.5 * pc(R2, ph)
+        assert rel_err(lhs, rhs) < 1e-13
