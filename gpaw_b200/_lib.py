@@ -51,6 +51,7 @@ SIGNATURES = {
                                                   ctypes.c_int, ctypes.c_double, _vp]),
     'gfd_operator_get_diagonal_element': (ctypes.c_int, [_vp, _dp]),
     'gfd_device_errors': (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    'gfd_poisson_set_rhs_operator': (ctypes.c_int, [_vp, _vp]),
     'gfd_preconditioner_create': (ctypes.c_int, [_vp] * 7 + [ctypes.c_int, ctypes.c_int64,
                                                              ctypes.POINTER(_vp)]),
     'gfd_preconditioner_destroy': (ctypes.c_int, [_vp]),

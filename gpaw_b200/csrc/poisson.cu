@@ -125,6 +125,7 @@ struct gfd_poisson {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int device = -1;
+  gfd_operator* B = nullptr;  // Mehrstellen right-hand side (not owned)
 };
 
 namespace gfd {
@@ -216,6 +217,20 @@ static int iterate2(gfd_poisson* ps, int l, bool final_norm, cudaStream_t s,
   return GFD_OK;
 }
 
+// Level-0 source: rho_in - background (gpaw/poisson.py:128-138) and, for
+// the Mehrstellen form, B applied to it (gpaw/poisson.py:196-199).
+static int rhs_launch(gfd_poisson* ps, cudaStream_t s) {
+  Level& L0 = ps->L[0];
+  const int64_t n0 = L0.n;
+  const bool fp64 = ps->precision == GFD_POISSON_FP64;
+  double* rho0 = fp64 ? static_cast<double*>(L0.rho) : ps->rho64;
+  double* dst = ps->B ? (fp64 ? static_cast<double*>(L0.res) : ps->r64) : rho0;
+  launch_k(sub_bg_kernel, grid_for(n0), 256, 0, s, dst, ps->rho_in, ps->dctrl, (long long)n0);
+  int st = check_launch("sub_bg_kernel");
+  if (st || !ps->B) return st;
+  return op_launch(ps->B, GFD_FLOAT64, OP_APPLY, dst, rho0, nullptr, 1, nullptr, 0.0, nullptr, s);
+}
+
 // Body of the solve loop: one iteration of the chosen form, ending with the
 // stopping-rule kernel.
 static int loop_body(gfd_poisson* ps, cudaGraphConditionalHandle loop, int in_graph,
@@ -281,9 +296,8 @@ static int capture_solve(gfd_poisson* ps, cudaStream_t cs, cudaGraph_t* body_out
                           &ps->dctrl->charge, cs)))
     return st;
   launch_k(prep_kernel, 1, 1, 0, cs, ps->dctrl, double(n0), ps->dv, loop, 1);
-  double* rho0 = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.rho) : ps->rho64;
-  launch_k(sub_bg_kernel, blocks, 256, 0, cs, rho0, ps->rho_in, ps->dctrl, (long long)n0);
-  if ((st = check_launch("prologue"))) return st;
+  if ((st = check_launch("prep_kernel"))) return st;
+  if ((st = rhs_launch(ps, cs))) return st;
   if (ps->precision == GFD_POISSON_MIXED &&
       (st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1, nullptr,
                       0.0, nullptr, cs)))
@@ -450,9 +464,8 @@ static int solve_eager(gfd_poisson* ps, cudaStream_t s) {
                           &ps->dctrl->charge, s)))
     return st;
   launch_k(prep_kernel, 1, 1, 0, s, ps->dctrl, double(n0), ps->dv, cudaGraphConditionalHandle(0), 0);
-  double* rho0 = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(L0.rho) : ps->rho64;
-  launch_k(sub_bg_kernel, blocks, 256, 0, s, rho0, ps->rho_in, ps->dctrl, n0);
-  if ((st = check_launch("prologue"))) return st;
+  if ((st = check_launch("prep_kernel"))) return st;
+  if ((st = rhs_launch(ps, s))) return st;
   if (ps->precision == GFD_POISSON_MIXED &&
       (st = op_launch(L0.op, GFD_FLOAT64, OP_RESIDUAL, ps->phi64, ps->r64, ps->rho64, 1, nullptr,
                       0.0, nullptr, s)))
@@ -606,6 +619,23 @@ extern "C" int gfd_poisson_destroy(gfd_poisson* ps) {
   if (ps->pool) cudaFree(ps->pool);
   if (ps->hctrl) cudaFreeHost(ps->hctrl);
   delete ps;
+  return GFD_OK;
+}
+
+extern "C" int gfd_poisson_set_rhs_operator(gfd_poisson* ps, gfd_operator* B) {
+  if (!ps) return set_error(GFD_EINVAL, "null solver");
+  if (B) {
+    const gfd_operator* A = ps->L[0].op;
+    if (!B->real) return set_error(GFD_EINVAL, "right-hand-side operator must be real");
+    if (B->n[0] != A->n[0] || B->n[1] != A->n[1] || B->n[2] != A->n[2])
+      return set_error(GFD_EINVAL, "right-hand-side operator is on another grid");
+  }
+  ps->B = B;
+  // The solve graph holds the old prologue: capture it again on the next solve.
+  if (ps->exec) cudaGraphExecDestroy(ps->exec);
+  if (ps->graph) cudaGraphDestroy(ps->graph);
+  ps->exec = nullptr;
+  ps->graph = nullptr;
   return GFD_OK;
 }
 

@@ -25,7 +25,7 @@ import numpy as np
 
 from . import _lib
 from .errors import PoissonConvergenceError  # noqa: F401  (re-exported)
-from .fd_operators import Laplace
+from .fd_operators import Laplace, LaplaceA, LaplaceB
 from .tensors import require_device, stream_of
 from .transformers import Transformer
 
@@ -55,12 +55,18 @@ class PoissonSolver:
         return self.nn
 
     def set_grid_descriptor(self, gd):
-        if self.nn == 'M':
-            raise NotImplementedError('Mehrstellen Poisson (nn="M") is not provided')
         self.gd = gd
         self.dv = gd.dv
         scale = -0.25 / pi
-        self.operators = [Laplace(gd, scale, self.nn, allocate=False)]
+        if self.nn == 'M':
+            # Mehrstellen: LaplaceA phi = LaplaceB rho (gpaw/poisson.py:53-59)
+            if not gd.orthogonal:
+                raise RuntimeError('Cannot use Mehrstellen stencil with non orthogonal cell.')
+            self.operators = [LaplaceA(gd, -scale, allocate=False)]
+            self.B = LaplaceB(gd, allocate=False)
+        else:
+            self.operators = [Laplace(gd, scale, self.nn, allocate=False)]
+            self.B = None
         self.interpolators = []
         self.restrictors = []
         self.presmooths = [2]
@@ -83,7 +89,8 @@ class PoissonSolver:
         self.levels = level
 
     def initialize(self, load_gauss=False):
-        for obj in self.operators + self.interpolators + self.restrictors:
+        extra = [self.B] if self.B is not None else []
+        for obj in self.operators + self.interpolators + self.restrictors + extra:
             if not obj.allocated:
                 obj.allocate()
         self.presmooths[self.levels] = 8
@@ -102,6 +109,9 @@ class PoissonSolver:
             L, ops, rs, ips, pre, post, w, self.relax_method, float(self.gd.dv),
             int(self.gd.pbc_c.all()), mode, _lib.ctypes.byref(handle)), 'PoissonSolver')
         self.solver = handle
+        if self.B is not None:
+            _lib.check(_lib.lib.gfd_poisson_set_rhs_operator(handle, self.B.operator),
+                       'PoissonSolver')
 
     def __del__(self):
         h = getattr(self, 'solver', None)

@@ -216,6 +216,14 @@ GFD_API int gfd_poisson_create(int levels, gfd_operator* const* ops, gfd_transfo
                        double dv, int pbc_all, int precision, gfd_poisson** ps);
 GFD_API int gfd_poisson_destroy(gfd_poisson* ps);
 
+/* Right-hand-side operator of the Mehrstellen solver (nn = 'M',
+ * gpaw/poisson.py:53-59): the level-0 source becomes B (rho - background),
+ * as solve_neutral applies self.B (gpaw/poisson.py:196-199); the level-0
+ * operator given to gfd_poisson_create is then LaplaceA.  B is borrowed, on
+ * the level-0 grid, real.  NULL removes it.  Batches built earlier keep the
+ * previous form. */
+GFD_API int gfd_poisson_set_rhs_operator(gfd_poisson* ps, gfd_operator* B);
+
 /* PoissonSolver.solve(phi, rho, charge=None, eps, maxcharge) for a charge-
  * neutral rho (gpaw/poisson.py:124-138, 193-218).  phi (in: initial guess,
  * out: solution) and rho are device float64 arrays of the fine grid.

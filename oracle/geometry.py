@@ -116,6 +116,30 @@ def laplace_stencil(gd, scale=1.0, n=1):
     return np.array(coefs, float), np.array(offsets, np.int64).reshape(-1, 3)
 
 
+def laplace_a_stencil(gd, scale):
+    """Mehrstellen left-hand operator LaplaceA (gpaw/fd_operators.py:192-216):
+    centre, six face neighbours and twelve edge neighbours of an orthogonal
+    cell (the module divides with true division)."""
+    c = (-1.0 / 12.0) / gd.h_cv.diagonal() ** 2 * scale
+    c0, c1, c2 = c[1] + c[2], c[0] + c[2], c[1] + c[0]
+    a = -16.0 * np.sum(c)
+    b = 10.0 * c + 0.125 * a
+    coefs = [a, b[0], b[0], b[1], b[1], b[2], b[2]] + [c0] * 4 + [c1] * 4 + [c2] * 4
+    offsets = [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1),
+               (0, -1, -1), (0, -1, 1), (0, 1, -1), (0, 1, 1),
+               (-1, 0, -1), (-1, 0, 1), (1, 0, -1), (1, 0, 1),
+               (-1, -1, 0), (-1, 1, 0), (1, -1, 0), (1, 1, 0)]
+    return np.array(coefs, float), np.array(offsets, np.int64)
+
+
+def laplace_b_stencil():
+    """Mehrstellen right-hand operator LaplaceB (gpaw/fd_operators.py:218-229)."""
+    b = 1.0 / 12.0
+    return (np.array([0.5, b, b, b, b, b, b]),
+            np.array([(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1),
+                      (0, 0, 1)], np.int64))
+
+
 def gradient_stencil(gd, v, scale=1.0, n=1):
     """Gradient coefficients/offsets (gpaw/fd_operators.py:123-144)."""
     h = (gd.h_cv ** 2).sum(1) ** 0.5

@@ -59,7 +59,7 @@ def _lib(impl):
                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
                                      ctypes.c_int]
         lib.ref_relax.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _lp, _lp, ctypes.c_int, _lp,
-                                  _dp, _dp, ctypes.c_int, ctypes.c_double]
+                                  ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_double]
         lib.ref_transform.argtypes = [_lp, _lp, ctypes.c_int, _lp, _lp, _lp, _lp, ctypes.c_int,
                                       ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]
     _libs[impl] = lib
@@ -143,8 +143,8 @@ def relax(method, coefs, offsets_pc, pbc_c, phi, rho, nsweeps, w, impl='port'):
         mp, flat, cfd = geometry.fd_layout(offsets_pc, n_c)
         nbr = np.where(np.asarray(pbc_c, bool).ravel()[:, None] * np.ones((3, 2), bool), 0, -1)
         st = lib.ref_relax(int(method), len(coefs), _ptr(coefs), _ptr(_cl(flat), _lp),
-                           _ptr(_cl(n_c), _lp), mp, _ptr(_cl(nbr), _lp), _ptr(phi), _ptr(rho),
-                           int(nsweeps), float(w))
+                           _ptr(_cl(n_c), _lp), mp, _ptr(_cl(nbr), _lp), int(cfd), _ptr(phi),
+                           _ptr(rho), int(nsweeps), float(w))
     _check(st, 'relax')
 
 

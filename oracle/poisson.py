@@ -37,7 +37,13 @@ class PoissonSolver:
         self.dv = gd.dv
         scale = -0.25 / pi
         self.grids = [gd]
-        self.stencils = [geometry.laplace_stencil(gd, scale, self.nn)]
+        if self.nn == 'M':
+            # Mehrstellen: A phi = B rho (gpaw/poisson.py:53-59)
+            self.stencils = [geometry.laplace_a_stencil(gd, -scale)]
+            self.B = geometry.laplace_b_stencil()
+        else:
+            self.stencils = [geometry.laplace_stencil(gd, scale, self.nn)]
+            self.B = None
         self.presmooths = [2]
         self.postsmooths = [1]
         self.weights = [2.0 / 3.0]
@@ -86,7 +92,12 @@ class PoissonSolver:
 
     def solve_neutral(self, phi, rho, eps=2e-10):
         self.phis[0] = phi
-        self.rhos[0][:] = rho
+        if self.B is None:
+            self.rhos[0][:] = rho
+        else:
+            # gpaw/poisson.py:196-199
+            self.rhos[0][:] = kernels.fd_apply(self.B[0], self.B[1], self.gd.pbc_c, rho,
+                                               impl=self.impl)
         niter = 1
         self.errors = []
         while self.iterate2() > eps and niter < self.maxiter:

@@ -109,12 +109,14 @@ int ref_fd_apply(int P, const double* coefs, const long* offsets, const long siz
 }
 
 int ref_relax(int relax_method, int P, const double* coefs, const long* offsets,
-              const long size[3], int range, const long neighbors[6], double* fun,
+              const long size[3], int range, const long neighbors[6], int cfd, double* fun,
               const double* src, int nrelax, double w) {
   bmgsstencil s = bmgs_stencil(P, coefs, offsets, range, size);
   const long padding[3][2] = {{range, range}, {range, range}, {range, range}};
+  /* The operator's own boundary object: cfd = 0 for stencils with cross
+     terms (gpaw/fd_operators.py:26-30), so corners are filled. */
   boundary_conditions* bc = bc_init(size, padding, padding,
-                                    (const long (*)[2])neighbors, MPI_COMM_NULL, 1, 1);
+                                    (const long (*)[2])neighbors, MPI_COMM_NULL, 1, cfd);
   const int* size2 = bc->size2;
   double* buf = (double*)malloc(sizeof(double) * size2[0] * size2[1] * size2[2]);
   double* sendbuf = (double*)malloc(sizeof(double) * (bc->maxsend + 1));

@@ -132,6 +132,29 @@ def main():
         d['ps_%s_niter' % tag] = np.array(niter)
         d['ps_%s_err' % tag] = np.array(ps.errors[-1])
 
+    # Mehrstellen Poisson (nn='M': LaplaceA phi = LaplaceB rho), Jacobi.
+    for tag, N, pbc in [('m16', 16, 0), ('m16p', 16, 1)]:
+        gd = grid((N, N, N), 0.2 / G.BOHR, pbc)
+        r = gd.coords()
+        L = gd.cell_cv.diagonal()
+        rho = np.zeros(tuple(gd.n_c))
+        for q in (1.0, -1.0):
+            R = rng.uniform(0.3, 0.7, 3) * L
+            s = 0.5 / G.BOHR
+            rho += q * np.exp(-sum((r[c] - R[c]) ** 2 for c in range(3)) / (2 * s * s))
+        rho -= rho.mean()
+        ps = P.PoissonSolver('M', 'J', 2e-10, impl='ref')
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        phi = np.zeros(tuple(gd.n_c))
+        niter = ps.solve(phi, rho)
+        d['mehr_%s_N' % tag] = gd.N_c
+        d['mehr_%s_pbc' % tag] = np.array([pbc] * 3)
+        d['mehr_%s_cell' % tag] = gd.cell_cv
+        d['mehr_%s_rho' % tag] = rho
+        d['mehr_%s_phi' % tag] = phi
+        d['mehr_%s_niter' % tag] = np.array(niter)
+
     np.savez_compressed(OUT, **d)
     print('wrote', OUT, os.path.getsize(OUT), 'bytes,', len(d), 'arrays')
 

@@ -155,3 +155,28 @@ def test_gauss_multipoles(cuda):
         phi, niter, err = solve_gpu(cuda, og, g[L])
         residual = np.sqrt(((phi - v[L]) ** 2).sum() * og.dv)
         assert residual < 0.6, (L, residual)
+
+
+@pytest.mark.parametrize('tag', ['m16', 'm16p'])
+def test_golden_mehrstellen_solve(golden, cuda, tag):
+    """nn='M' (LaplaceA phi = LaplaceB rho) against the solve run on the
+    reference's own C kernels: same V-cycle count, potential within 1e-10."""
+    d = golden
+    og = G.Grid(d['mehr_%s_N' % tag], d['mehr_%s_cell' % tag], d['mehr_%s_pbc' % tag])
+    phi, niter, err = solve_gpu(cuda, og, d['mehr_%s_rho' % tag], 'M')
+    assert niter == int(d['mehr_%s_niter' % tag])
+    assert np.abs(phi - d['mehr_%s_phi' % tag]).max() < 1e-10
+    assert err <= 2e-10
+
+
+@pytest.mark.parametrize('pbc', [0, 1])
+def test_mehrstellen_matches_oracle(cuda, pbc):
+    og = G.Grid((48,) * 3, (48 * 0.2 / BOHR,) * 3, pbc)
+    rho = gaussians_rho(og, 16, 5)
+    phi_o, n_o, err_o = solve_oracle(og, rho, 'M')
+    phi, niter, err = solve_gpu(cuda, og, rho, 'M')
+    assert niter == n_o
+    assert np.abs(phi - phi_o).max() < 1e-10
+    phi_m, n_m, err_m = solve_gpu(cuda, og, rho, 'M', precision='mixed')
+    assert err_m <= 2e-10
+    assert np.abs(phi_m - phi_o).max() < 1e-9

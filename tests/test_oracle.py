@@ -201,3 +201,35 @@ def test_oracle_preconditioner_is_linear():
         lhs = pc(2.0 * R1 - 0.5 * R2, ph)
         rhs = 2.0 * pc(R1, ph) - 0.5 * pc(R2, ph)
         assert rel_err(lhs, rhs) < 1e-13
+
+
+@pytest.mark.parametrize('tag', ['m16', 'm16p'])
+def test_mehrstellen_poisson_matches_golden(golden, tag):
+    """nn='M' (LaplaceA phi = LaplaceB rho, gpaw/poisson.py:53-59, 196-199)
+    against the solve run on the reference's own C kernels."""
+    d = golden
+    gd = _grid(d, 'mehr_' + tag)
+    ps = P.PoissonSolver('M', 'J', 2e-10)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    phi = np.zeros(tuple(gd.n_c))
+    niter = ps.solve(phi, d['mehr_%s_rho' % tag])
+    assert niter == int(d['mehr_%s_niter' % tag])
+    assert np.abs(phi - d['mehr_%s_phi' % tag]).max() < 1e-13
+
+
+@pytest.mark.skipif(not K.have_ref(), reason='reference library not built here')
+def test_cross_term_relax_port_equals_reference():
+    """Relaxation with a cross-term stencil (LaplaceA: the operator's cfd flag
+    is 0, so halo corners are filled) bit for bit against GPAW's C."""
+    rng = np.random.default_rng(6)
+    for pbc in (0, 1, (1, 0, 1)):
+        gd = G.Grid((12, 10, 14), (3.0, 2.5, 3.5), pbc)
+        c, o = G.laplace_a_stencil(gd, 0.25 / pi)
+        a = rng.standard_normal(tuple(gd.n_c))
+        rho = rng.standard_normal(tuple(gd.n_c))
+        for method, w in ((2, 2.0 / 3.0), (1, 1.0)):
+            p1, p2 = a.copy(), a.copy()
+            K.relax(method, c, o, gd.pbc_c, p1, rho, 2, w)
+            K.relax(method, c, o, gd.pbc_c, p2, rho, 2, w, impl='ref')
+            assert np.array_equal(p1, p2), (pbc, method)
