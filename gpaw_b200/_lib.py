@@ -51,6 +51,8 @@ SIGNATURES = {
                                                   ctypes.c_int, ctypes.c_double, _vp]),
     'gfd_operator_get_diagonal_element': (ctypes.c_int, [_vp, _dp]),
     'gfd_device_errors': (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    'gfd_density_interpolate': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_int, _vp]),
     'gfd_poisson_set_rhs_operator': (ctypes.c_int, [_vp, _vp]),
     'gfd_preconditioner_create': (ctypes.c_int, [_vp] * 7 + [ctypes.c_int, ctypes.c_int64,
                                                              ctypes.POINTER(_vp)]),

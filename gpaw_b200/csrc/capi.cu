@@ -1,5 +1,6 @@
 // capi.cu -- error reporting, device queries, reductions and small streaming
 // launches of libgpawfd.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -200,6 +201,37 @@ extern "C" size_t gfd_last_error(char* buf, size_t len) {
 }
 
 extern "C" const char* gfd_version(void) { return "gpaw-fd-b200 0.1 sm_100a"; }
+
+extern "C" int gfd_density_interpolate(gfd_transformer* tr, const double* nt_sG, double* nt_sg,
+                                       int64_t nspins, double pseudo_charge, double dv_fine,
+                                       int renormalize, void* stream) {
+  if (!tr) return set_error(GFD_EINVAL, "null transformer");
+  if (!tr->interpolate) return set_error(GFD_EINVAL, "the transformer must interpolate");
+  if (!tr->real) return set_error(GFD_EINVAL, "densities are real");
+  if (nspins < 0) return set_error(GFD_EINVAL, "negative spin count");
+  if (nspins == 0) return GFD_OK;
+  if (!nt_sG || !nt_sg) return set_error(GFD_EINVAL, "null array pointer");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st = tr_launch(tr, GFD_FLOAT64, nt_sG, nt_sg, nspins, nullptr, s);
+  if (st) return st;
+  // gpaw/density.py:229-235: only with a zero boundary on some axis and a
+  // nonzero pseudo charge.
+  if (!renormalize || std::fabs(pseudo_charge) <= 1.0e-14) return GFD_OK;
+  const int64_t n = (int64_t)tr->nout[0] * tr->nout[1] * tr->nout[2] * nspins;
+  double* buf = nullptr;
+  if ((st = check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&buf),
+                                       sizeof(double) * (kRedBlocks + 1), s),
+                       "cudaMallocAsync(reduction)")))
+    return st;
+  st = reduce_launch(GFD_FLOAT64, nt_sg, n, false, dv_fine, buf, buf + kRedBlocks, s);
+  if (!st) {
+    launch_k(scale_to_total_kernel, grid_for(n), 256, 0, s, nt_sg, (long long)n, pseudo_charge,
+             (const double*)(buf + kRedBlocks));
+    st = check_launch("scale_to_total_kernel");
+  }
+  cudaFreeAsync(buf, s);
+  return st;
+}
 
 extern "C" int gfd_grid_sum(const double* a, int64_t n, double scale, double* result,
                             void* stream) {

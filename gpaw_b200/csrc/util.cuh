@@ -70,6 +70,18 @@ __global__ void __launch_bounds__(256) add_potential_kernel(V* __restrict__ out,
   }
 }
 
+// y[i] *= target / *total (total on the device, computed by an earlier
+// kernel on the stream).
+static __global__ void __launch_bounds__(256) scale_to_total_kernel(double* __restrict__ y, long long n,
+                                                             double target,
+                                                             const double* __restrict__ total) {
+  pdl_enter();
+  const double x = target / *total;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] *= x;
+}
+
 // Per-block partial sums of a[i] (SQUARE: a[i]^2), in a fixed order.
 template <class T, bool SQUARE>
 __global__ void __launch_bounds__(kRedThreads) partial_sum_kernel(const T* __restrict__ a,

@@ -168,6 +168,16 @@ GFD_API int gfd_preconditioner_destroy(gfd_preconditioner* pc);
 GFD_API int gfd_preconditioner_apply(gfd_preconditioner* pc, int dtype, const void* residuals,
                                      void* out, int64_t nb, const double* phase_cd, void* stream);
 
+/* Pseudo density to the fine grid: Density.interpolate
+ * (gpaw/density.py:217-235).  nt_sg = interpolate(nt_sG) for nspins real
+ * grids; then, when renormalize != 0 (the caller's "not all periodic") and
+ * |pseudo_charge| > 1e-14, nt_sg *= pseudo_charge / (dv_fine * sum(nt_sg)),
+ * the reference's x = pseudo_charge / finegd.integrate(nt_sg).sum().  The
+ * sum stays on the device; the host does not wait. */
+GFD_API int gfd_density_interpolate(gfd_transformer* tr, const double* nt_sG, double* nt_sg,
+                                    int64_t nspins, double pseudo_charge, double dv_fine,
+                                    int renormalize, void* stream);
+
 /* Device-side error flags of the current device, then cleared: *flags != 0
  * when a stencil kernel gave up on a bounded wait since the last call (its
  * output is then incomplete).  No counterpart in the reference, whose CPU

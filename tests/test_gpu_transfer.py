@@ -111,3 +111,30 @@ def test_batched_bands_112(cuda):
     back = torch.empty_like(t)
     rs.apply(fine_t, back)
     assert rel_err(host(back), K.transform(of, oc, 3, ref_f, nthreads=8)) < TOL
+
+
+@pytest.mark.parametrize('pbc', [0, (1, 0, 1), 1])
+def test_pseudo_density_interpolation(cuda, pbc):
+    """Density.interpolate (gpaw/density.py:217-235): two spins to the fine
+    grid with nn = 3, renormalised to the pseudo charge unless every axis is
+    periodic; against the oracle interpolation and the reference's formula."""
+    import torch
+    from gpaw_b200.density import interpolate_pseudo_density
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.transformers import Transformer
+    og = G.Grid((24, 20, 28), (24 * 0.35, 20 * 0.35, 28 * 0.35), pbc)
+    of = og.refine()
+    gd = product_grid(og)
+    fine = gd.refine()
+    rng = np.random.default_rng(17)
+    nt = rng.uniform(0, 1, (2,) + tuple(og.n_c))
+    pseudo_charge = -3.75
+    ref = K.transform(og, of, 3, nt, nthreads=8)
+    if not og.pbc_c.all():
+        ref = ref * (pseudo_charge / of.integrate(ref).sum())
+    out = torch.empty((2,) + tuple(int(x) for x in fine.n_c), dtype=torch.float64, device=cuda)
+    interpolate_pseudo_density(Transformer(gd, fine, 3), dev(nt, cuda), out, fine, pseudo_charge)
+    torch.cuda.synchronize()
+    assert rel_err(host(out), ref) < TOL
+    if not og.pbc_c.all():
+        assert abs(of.integrate(host(out)).sum() - pseudo_charge) < 1e-12
