@@ -84,6 +84,13 @@ __device__ __forceinline__ cplx<float> ldro(const cplx<float>* p) {
   return {v.x, v.y};
 }
 
+// Load policy of the per-point functions (stencil.cuh, transfer.cuh): the
+// read-only path.
+struct LoadRO {
+  template <class T>
+  __device__ __forceinline__ static T ld(const T* p) { return ldro(p); }
+};
+
 // Streaming store (output is not re-read by this kernel).
 __device__ __forceinline__ void stcs(double* p, double v) { __stcs(p, v); }
 __device__ __forceinline__ void stcs(float* p, float v) { __stcs(p, v); }

@@ -394,57 +394,72 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
 // nin * n0 * n1 * n2 points with a fixed grid, so the per-CTA partial sums
 // of MODE_RESIDUAL have a fixed order.
 // ---------------------------------------------------------------------------
+// One output point of the direct star stencil at (i0, i1, i2) of a band:
+// base / rho_b point to the band, rem = (i0 n1 + i1) n2 + i2.  Every mode;
+// LD is the load policy (common.cuh).
+template <class V, int R, int MODE, class LD>
+__device__ __forceinline__ V star_point_at(const V* __restrict__ base, const V* __restrict__ rho_b,
+                                           const StarParams<typename vt<V>::S>& p, int i0, int i1,
+                                           int i2, long long rem) {
+  using Sc = typename vt<V>::S;
+  const long long plane = (long long)p.n1 * p.n2;
+  const int r1 = int(rem - i0 * plane);
+  Sc cc = p.c0;
+  if constexpr (MODE == MODE_POTENTIAL) cc += LD::ld(static_cast<const Sc*>(p.pot) + rem);
+  V s = vmul(cc, LD::ld(base + rem));
+#pragma unroll
+  for (int k = -R; k <= R; k++) {
+    if (k == 0) continue;
+    int sd;
+    int j = wrap_axis(i0 + k, p.n0, p.per0, sd);
+    if (j >= 0) {
+      V v = LD::ld(base + j * plane + r1);
+      if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 0, sd), v); }
+      madd(s, p.cx[kMaxR + k], v);
+    }
+    j = wrap_axis(i1 + k, p.n1, p.per1, sd);
+    if (j >= 0) {
+      V v = LD::ld(base + i0 * plane + j * p.n2 + i2);
+      if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 1, sd), v); }
+      madd(s, p.cy[kMaxR + k], v);
+    }
+    j = wrap_axis(i2 + k, p.n2, p.per2, sd);
+    if (j >= 0) {
+      V v = LD::ld(base + i0 * plane + i1 * p.n2 + j);
+      if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 2, sd), v); }
+      madd(s, p.cz[kMaxR + k], v);
+    }
+  }
+  if constexpr (MODE == MODE_JACOBI) return vmul(p.wc, vsub(LD::ld(rho_b + rem), s));
+  else if constexpr (MODE == MODE_RESIDUAL) return vsub(s, LD::ld(rho_b + rem));
+  else return s;
+}
+
+// The same at flat index g over all bands.
+template <class V, int R, int MODE, class LD>
+__device__ __forceinline__ V star_point(const V* __restrict__ in, const V* __restrict__ rho,
+                                        const StarParams<typename vt<V>::S>& p, long long g) {
+  const long long plane = (long long)p.n1 * p.n2;
+  const long long b = g / p.band;
+  const long long rem = g - b * p.band;
+  const int i0 = int(rem / plane);
+  const int r1 = int(rem - i0 * plane);
+  const int i1 = r1 / p.n2, i2 = r1 - i1 * p.n2;
+  return star_point_at<V, R, MODE, LD>(in + b * p.band, rho ? rho + b * p.band : nullptr, p, i0,
+                                       i1, i2, rem);
+}
+
 template <class V, int R, int MODE>
 __global__ void __launch_bounds__(256)
 star_direct_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
                    const StarParams<typename vt<V>::S> p, long long total) {
   pdl_enter();
-  using Sc = typename vt<V>::S;
   __shared__ double red[8];
-  const long long plane = (long long)p.n1 * p.n2;
   double sumsq = 0.0;
   for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256) {
-    const long long b = g / p.band;
-    const long long rem = g - b * p.band;
-    const int i0 = int(rem / plane);
-    const int r1 = int(rem - i0 * plane);
-    const int i1 = r1 / p.n2, i2 = r1 - i1 * p.n2;
-    const V* base = in + b * p.band;
-    Sc cc = p.c0;
-    if constexpr (MODE == MODE_POTENTIAL) cc += ldro(static_cast<const Sc*>(p.pot) + rem);
-    V s = vmul(cc, ldro(in + g));
-#pragma unroll
-    for (int k = -R; k <= R; k++) {
-      if (k == 0) continue;
-      int sd;
-      int j = wrap_axis(i0 + k, p.n0, p.per0, sd);
-      if (j >= 0) {
-        V v = ldro(base + j * plane + r1);
-        if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 0, sd), v); }
-        madd(s, p.cx[kMaxR + k], v);
-      }
-      j = wrap_axis(i1 + k, p.n1, p.per1, sd);
-      if (j >= 0) {
-        V v = ldro(base + i0 * plane + j * p.n2 + i2);
-        if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 1, sd), v); }
-        madd(s, p.cy[kMaxR + k], v);
-      }
-      j = wrap_axis(i2 + k, p.n2, p.per2, sd);
-      if (j >= 0) {
-        V v = ldro(base + i0 * plane + i1 * p.n2 + j);
-        if constexpr (vt<V>::NC == 2) { if (sd >= 0) v = phase_mul(phase_of(p.P, 2, sd), v); }
-        madd(s, p.cz[kMaxR + k], v);
-      }
-    }
-    if constexpr (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) {
-      out[g] = s;
-    } else if constexpr (MODE == MODE_JACOBI) {
-      out[g] = vmul(p.wc, vsub(ldro(rho + g), s));
-    } else {
-      const V r = vsub(s, ldro(rho + g));
-      out[g] = r;
-      if constexpr (vt<V>::NC == 1) sumsq += sq(r);
-    }
+    const V o = star_point<V, R, MODE, LoadRO>(in, rho, p, g);
+    out[g] = o;
+    if constexpr (MODE == MODE_RESIDUAL && vt<V>::NC == 1) sumsq += sq(o);
   }
   if constexpr (MODE == MODE_RESIDUAL) {
     if (p.partials) {

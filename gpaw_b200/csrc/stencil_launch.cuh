@@ -239,12 +239,13 @@ int direct_dispatch(const gfd_operator* op, const V* in, V* out, const V* rho,
   return check_launch("star_direct_kernel");
 }
 
-template <class V>
-int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* out, const void* rho,
-                      int64_t nin, const double* phase_cd, double w, double* partials,
-                      cudaStream_t s) {
-  using S = typename vt<V>::S;
-  StarParams<S> p{};
+// Stencil parameters of a star operator for one mode (weights in the
+// element precision S; Jacobi folds (1 - w) phi into the centre weight, see
+// star_kernel, and the negated sweep flips the sign of w / c0, exactly).
+template <class S>
+void star_params(const gfd_operator* op, int mode, double w, const double* phase_cd,
+                 StarParams<S>& p) {
+  p = StarParams<S>{};
   p.n0 = op->n[0]; p.n1 = op->n[1]; p.n2 = op->n[2];
   p.per0 = op->per[0]; p.per1 = op->per[1]; p.per2 = op->per[2];
   p.band = (long long)op->n[0] * op->n[1] * op->n[2];
@@ -255,8 +256,6 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
     p.cz[i] = S(op->cz[i]);
   }
   if (mode == OP_JACOBI || mode == OP_JACOBI_NEG) {
-    // Fold (1 - w) phi into the centre weight (see star_kernel); the
-    // negated sweep flips the sign of w / c0, which is exact.
     p.c0 = S(-(1.0 - w) * op->c0 / w);
     p.wc = S(w / op->c0);
     if (mode == OP_JACOBI_NEG) p.wc = -p.wc;
@@ -268,6 +267,15 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
       for (int d = 0; d < 2; d++)
         if (op->per[c] && (phase_cd[4 * c + 2 * d] != 1.0 || phase_cd[4 * c + 2 * d + 1] != 0.0))
           p.fix_yz = 1;
+}
+
+template <class V>
+int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* out, const void* rho,
+                      int64_t nin, const double* phase_cd, double w, double* partials,
+                      cudaStream_t s) {
+  using S = typename vt<V>::S;
+  StarParams<S> p;
+  star_params(op, mode, w, phase_cd, p);
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
   const V* vrho = static_cast<const V*>(rho);

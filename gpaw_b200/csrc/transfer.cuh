@@ -20,6 +20,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "internal.h"
 
 namespace gfd {
 
@@ -75,6 +76,28 @@ struct TrParams {
   // the band preconditioner; multiplying by -1 is exact).
   S out_scale;
 };
+
+// Transfer parameters of a transformer (host side).
+template <class S>
+void tr_params(const gfd_transformer* tr, const double* ph, void* seed, double seed_scale,
+               double out_scale, TrParams<S>& p) {
+  p = TrParams<S>{};
+  p.ni0 = tr->nin[0]; p.ni1 = tr->nin[1]; p.ni2 = tr->nin[2];
+  p.no0 = tr->nout[0]; p.no1 = tr->nout[1]; p.no2 = tr->nout[2];
+  p.lo0 = tr->pad[0][0]; p.lo1 = tr->pad[1][0]; p.lo2 = tr->pad[2][0];
+  p.sk0 = tr->skip[0][0]; p.sk1 = tr->skip[1][0]; p.sk2 = tr->skip[2][0];
+  p.per0 = tr->per[0]; p.per1 = tr->per[1]; p.per2 = tr->per[2];
+  p.band_in = (long long)tr->nin[0] * tr->nin[1] * tr->nin[2];
+  p.band_out = (long long)tr->nout[0] * tr->nout[1] * tr->nout[2];
+  for (int c = 0; c < 3; c++)
+    for (int d = 0; d < 2; d++) {
+      p.P.ph[c][d].re = ph ? S(ph[4 * c + 2 * d]) : S(1);
+      p.P.ph[c][d].im = ph ? S(ph[4 * c + 2 * d + 1]) : S(0);
+    }
+  p.seed = seed;
+  p.seed_scale = S(seed_scale);
+  p.out_scale = S(out_scale);
+}
 
 // Pack an in-plane source offset and its wrap sides; -1 = zero point.
 __device__ __forceinline__ int pack_src(int ys, int zs, int n2, int ysd, int zsd) {
@@ -343,14 +366,14 @@ interp_kernel(const V* __restrict__ in, V* out, const V* base,
 // the L1 cache.  The marching kernels above pay a memory round trip per plane,
 // which dominates on grids of a few thousand points.
 // ---------------------------------------------------------------------------
-template <class V, class S>
+template <class LD, class V, class S>
 __device__ __forceinline__ V tr_fetch(const V* base, int x, int y, int z, const TrParams<S>& p) {
   int sx, sy, sz;
   const int i = wrap_axis(x, p.ni0, p.per0, sx);
   const int j = wrap_axis(y, p.ni1, p.per1, sy);
   const int k = wrap_axis(z, p.ni2, p.per2, sz);
   if (i < 0 || j < 0 || k < 0) return vzero<V>();
-  V v = ldro(base + ((long long)i * p.ni1 + j) * p.ni2 + k);
+  V v = LD::ld(base + ((long long)i * p.ni1 + j) * p.ni2 + k);
   if constexpr (vt<V>::NC == 2) {
     if (sx >= 0) v = phase_mul(phase_of(p.P, 0, sx), v);
     if (sy >= 0) v = phase_mul(phase_of(p.P, 1, sy), v);
@@ -359,28 +382,78 @@ __device__ __forceinline__ V tr_fetch(const V* base, int x, int y, int z, const 
   return v;
 }
 
+// One restricted point at output coordinates (X, Y, Z) of a band (base:
+// the band's input), times out_scale; LD is the load policy (common.cuh).
+template <class V, int NN, class LD>
+__device__ __forceinline__ V restrict_point_at(const V* __restrict__ base, int X, int Y, int Z,
+                                               const TrParams<typename vt<V>::S>& p) {
+  constexpr int W = 2 * NN - 1;
+  // fine centre of each axis: 2i + (2nn-1) - lo
+  const int fx = 2 * X + W - p.lo0, fy = 2 * Y + W - p.lo1, fz = 2 * Z + W - p.lo2;
+  V v = rst_tap<NN, V>([&](int ox) {
+    return rst_tap<NN, V>([&](int oy) {
+      return rst_tap<NN, V>([&](int oz) { return tr_fetch<LD>(base, fx + ox, fy + oy, fz + oz, p); });
+    });
+  });
+  if (p.out_scale != typename vt<V>::S(1)) v = vmul(p.out_scale, v);
+  return v;
+}
+
+// The same at flat index g over all output bands.
+template <class V, int NN, class LD>
+__device__ __forceinline__ V restrict_point(const V* __restrict__ in,
+                                            const TrParams<typename vt<V>::S>& p, long long g) {
+  const long long plane_out = (long long)p.no1 * p.no2;
+  const long long b = g / p.band_out;
+  const long long rem = g - b * p.band_out;
+  const int X = int(rem / plane_out);
+  const int r1 = int(rem - X * plane_out);
+  const int Y = r1 / p.no2, Z = r1 - Y * p.no2;
+  return restrict_point_at<V, NN, LD>(in + b * p.band_in, X, Y, Z, p);
+}
+
+// One interpolated point at output coordinates (X, Y, Z), times out_scale
+// (SUB: *bo, the base value at that point, minus it).
+template <class V, int NN, bool SUB, class LD>
+__device__ __forceinline__ V interp_point_at(const V* __restrict__ base, const V* bo, int X, int Y,
+                                             int Z, const TrParams<typename vt<V>::S>& p) {
+  // g = f + skip[c][0]; even g: coarse point c(i) = i + nn - 1 - lo, odd: between c(i), c(i)+1
+  const int gx = X + p.sk0, gy = Y + p.sk1, gz = Z + p.sk2;
+  const int cx = (gx >> 1) + NN - 1 - p.lo0, cy = (gy >> 1) + NN - 1 - p.lo1,
+            cz = (gz >> 1) + NN - 1 - p.lo2;
+  auto along = [&](int odd, auto get) -> V { return odd ? ip_tap<NN, V>(get) : get(0); };
+  V v = along(gx & 1, [&](int ox) {
+    return along(gy & 1, [&](int oy) {
+      return along(gz & 1, [&](int oz) { return tr_fetch<LD>(base, cx + ox, cy + oy, cz + oz, p); });
+    });
+  });
+  if (p.out_scale != typename vt<V>::S(1)) v = vmul(p.out_scale, v);
+  // bo may be the output itself (in-place correction): a plain load.
+  if constexpr (SUB) v = vsub(*bo, v);
+  return v;
+}
+
+// The same at flat index g over all output bands.
+template <class V, int NN, bool SUB, class LD>
+__device__ __forceinline__ V interp_point(const V* __restrict__ in, const V* base_out,
+                                          const TrParams<typename vt<V>::S>& p, long long g) {
+  const long long plane_out = (long long)p.no1 * p.no2;
+  const long long b = g / p.band_out;
+  const long long rem = g - b * p.band_out;
+  const int X = int(rem / plane_out);
+  const int r1 = int(rem - X * plane_out);
+  const int Y = r1 / p.no2, Z = r1 - Y * p.no2;
+  return interp_point_at<V, NN, SUB, LD>(in + b * p.band_in, SUB ? base_out + g : nullptr, X, Y,
+                                         Z, p);
+}
+
 template <class V, int NN>
 __global__ void __launch_bounds__(256)
 restrict_direct_kernel(const V* __restrict__ in, V* __restrict__ out,
                        const TrParams<typename vt<V>::S> p, long long total) {
   pdl_enter();
-  constexpr int W = 2 * NN - 1;
-  const long long plane_out = (long long)p.no1 * p.no2;
   for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256) {
-    const long long b = g / p.band_out;
-    const long long rem = g - b * p.band_out;
-    const int X = int(rem / plane_out);
-    const int r1 = int(rem - X * plane_out);
-    const int Y = r1 / p.no2, Z = r1 - Y * p.no2;
-    const V* base = in + b * p.band_in;
-    // fine centre of each axis: 2i + (2nn-1) - lo
-    const int fx = 2 * X + W - p.lo0, fy = 2 * Y + W - p.lo1, fz = 2 * Z + W - p.lo2;
-    V v = rst_tap<NN, V>([&](int ox) {
-      return rst_tap<NN, V>([&](int oy) {
-        return rst_tap<NN, V>([&](int oz) { return tr_fetch(base, fx + ox, fy + oy, fz + oz, p); });
-      });
-    });
-    if (p.out_scale != typename vt<V>::S(1)) v = vmul(p.out_scale, v);
+    const V v = restrict_point<V, NN, LoadRO>(in, p, g);
     out[g] = v;
     if (p.seed) static_cast<V*>(p.seed)[g] = vmul(p.seed_scale, v);
   }
@@ -391,28 +464,8 @@ __global__ void __launch_bounds__(256)
 interp_direct_kernel(const V* __restrict__ in, V* out, const V* base_out,
                      const TrParams<typename vt<V>::S> p, long long total) {
   pdl_enter();
-  const long long plane_out = (long long)p.no1 * p.no2;
-  for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256) {
-    const long long b = g / p.band_out;
-    const long long rem = g - b * p.band_out;
-    const int X = int(rem / plane_out);
-    const int r1 = int(rem - X * plane_out);
-    const int Y = r1 / p.no2, Z = r1 - Y * p.no2;
-    const V* base = in + b * p.band_in;
-    // g = f + skip[c][0]; even g: coarse point c(i) = i + nn - 1 - lo, odd: between c(i), c(i)+1
-    const int gx = X + p.sk0, gy = Y + p.sk1, gz = Z + p.sk2;
-    const int cx = (gx >> 1) + NN - 1 - p.lo0, cy = (gy >> 1) + NN - 1 - p.lo1,
-              cz = (gz >> 1) + NN - 1 - p.lo2;
-    auto along = [&](int odd, auto get) -> V { return odd ? ip_tap<NN, V>(get) : get(0); };
-    V v = along(gx & 1, [&](int ox) {
-      return along(gy & 1, [&](int oy) {
-        return along(gz & 1, [&](int oz) { return tr_fetch(base, cx + ox, cy + oy, cz + oz, p); });
-      });
-    });
-    if (p.out_scale != typename vt<V>::S(1)) v = vmul(p.out_scale, v);
-    if constexpr (SUB) v = vsub(base_out[g], v);
-    out[g] = v;
-  }
+  for (long long g = blockIdx.x * 256LL + threadIdx.x; g < total; g += (long long)gridDim.x * 256)
+    out[g] = interp_point<V, NN, SUB, LoadRO>(in, base_out, p, g);
 }
 
 }  // namespace gfd

@@ -10,15 +10,6 @@
 
 namespace gfd {
 
-template <class S>
-static void fill_tr_phases(Phases<S>& P, const double* ph) {
-  for (int c = 0; c < 3; c++)
-    for (int d = 0; d < 2; d++) {
-      P.ph[c][d].re = ph ? S(ph[4 * c + 2 * d]) : S(1);
-      P.ph[c][d].im = ph ? S(ph[4 * c + 2 * d + 1]) : S(0);
-    }
-}
-
 template <class V, int NN>
 static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t nin,
                        TrParams<typename vt<V>::S>& p, cudaStream_t s) {
@@ -94,18 +85,8 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const 
                     int64_t nin, const double* ph, cudaStream_t s, void* seed = nullptr,
                     double seed_scale = 0.0, double out_scale = 1.0) {
   using S = typename vt<V>::S;
-  TrParams<S> p{};
-  p.ni0 = tr->nin[0]; p.ni1 = tr->nin[1]; p.ni2 = tr->nin[2];
-  p.no0 = tr->nout[0]; p.no1 = tr->nout[1]; p.no2 = tr->nout[2];
-  p.lo0 = tr->pad[0][0]; p.lo1 = tr->pad[1][0]; p.lo2 = tr->pad[2][0];
-  p.sk0 = tr->skip[0][0]; p.sk1 = tr->skip[1][0]; p.sk2 = tr->skip[2][0];
-  p.per0 = tr->per[0]; p.per1 = tr->per[1]; p.per2 = tr->per[2];
-  p.band_in = (long long)tr->nin[0] * tr->nin[1] * tr->nin[2];
-  p.band_out = (long long)tr->nout[0] * tr->nout[1] * tr->nout[2];
-  fill_tr_phases(p.P, ph);
-  p.seed = seed;
-  p.seed_scale = S(seed_scale);
-  p.out_scale = S(out_scale);
+  TrParams<S> p;
+  tr_params(tr, ph, seed, seed_scale, out_scale, p);
   if (seed && tr->interpolate) return set_error(GFD_EINVAL, "seeded form is for restriction only");
   const V* vin = static_cast<const V*>(in);
   V* vout = static_cast<V*>(out);
