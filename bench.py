@@ -550,9 +550,15 @@ def run_gpu_arm(args):
     if args.e2e_steps > 0:
         from gpaw_b200.streaming import HostStreamer
         e2e_steps = min(args.steps, args.e2e_steps)
-        host_in = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+        try:
+            host_in = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+            host_out = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+            pinned = True
+        except RuntimeError:  # page-locking refused (memlock limit): pageable copies
+            host_in = torch.empty(shape, dtype=torch.complex128)
+            host_out = torch.empty(shape, dtype=torch.complex128)
+            pinned = False
         host_in.copy_(a)
-        host_out = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
         streamer = HostStreamer(lap, chunk_bands=16)
         streamer.apply(host_in, host_out, phase)  # warm-up (device buffers)
         torch.cuda.synchronize()
@@ -568,7 +574,8 @@ def run_gpu_arm(args):
         e2e = {'value': world * nbytes / (e2e_ms * 1e-3) / 1e9, 'unit': 'GB/s',
                'steps': e2e_steps, 'h2d_bytes_per_step': nbytes // 2,
                'd2h_bytes_per_step': nbytes // 2,
-               'api': 'gpaw_b200.streaming.HostStreamer.apply, 16-band chunks'}
+               'api': 'gpaw_b200.streaming.HostStreamer.apply, 16-band chunks',
+               'pinned_host_memory': pinned}
         del host_in, host_out, streamer
 
     ham = pcb = None
