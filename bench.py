@@ -300,7 +300,8 @@ def poisson_bench(nsolves=8):
 SERVING_SIZES = (32, 48, 64, 96, 128, 160)
 
 
-def serving_bench(rates=(1000.0, 5000.0), nreq=300, precisions=('fp64', 'mixed'), seed=5):
+def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=300,
+                  precisions=('fp64', 'mixed'), seed=5):
     import torch
     from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
     h = 0.2 / BOHR
@@ -426,6 +427,58 @@ def hamiltonian_bench(lap, a, b, phase, steps):
             'fused_ms': fused_ms, 'fused_GBps': nbytes / (fused_ms * 1e-3) / 1e9,
             'two_pass_ms': two_ms, 'speedup_vs_two_pass': two_ms / fused_ms,
             'bytes_per_point': BYTES_PER_POINT}
+
+
+# ---------------------------------------------------------------------------
+# The rest of the stencil configurations: Gradient(v, 1.0, n=3) on the
+# headline bands, the complex64 (FP32) copy of the Laplace workload, and the
+# plain FP64 Laplace of 16 x 47^3 (too small for bandwidth: its latency).
+# ---------------------------------------------------------------------------
+def stencil_variants_bench(gd, a, b, phase, steps):
+    import torch
+    from gpaw_b200.fd_operators import Gradient, Laplace
+    from gpaw_b200.grid_descriptor import GridDescriptor
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {}
+    nbytes = BYTES_PER_POINT * a.numel()
+    for v in range(3):
+        grad = Gradient(gd, v, 1.0, 3, complex)
+        ms = timed(lambda: grad.apply(a, b, phase), steps)
+        out['gradient%d_GBps' % v] = nbytes / (ms * 1e-3) / 1e9
+    lap32 = Laplace(gd, -0.5, 3, np.complex64)
+    a32 = a.to(torch.complex64)
+    b32 = torch.empty_like(a32)
+    ms = timed(lambda: lap32.apply(a32, b32, phase), steps)
+    out['complex64_laplace_GBps'] = 16 * a32.numel() / (ms * 1e-3) / 1e9
+    del a32, b32
+    N1 = 48
+    gd1 = GridDescriptor((N1,) * 3, (N1 * 0.2 / BOHR,) * 3, 0)
+    lap1 = Laplace(gd1, -0.5, 3)
+    g = torch.Generator(device='cuda')
+    g.manual_seed(1)
+    x = torch.rand((16,) + tuple(int(n) for n in gd1.n_c), dtype=torch.float64, device='cuda',
+                   generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    ms = timed(lambda: lap1.apply(x, y), 200)
+    out['plain_fp64_16x47_us'] = ms * 1e3
+    out['plain_fp64_16x47_GBps'] = 16 * x.numel() / (ms * 1e-3) / 1e9
+    out['workload'] = ('Gradient v=0,1,2 and complex64 Laplace on %d bands x 96^3 (32 / 16 B '
+                       'per point); float64 Laplace nn=3 on 16 x 47^3 zero boundary'
+                       % a.shape[0])
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -578,10 +631,11 @@ def run_gpu_arm(args):
                'pinned_host_memory': pinned}
         del host_in, host_out, streamer
 
-    ham = pcb = None
+    ham = pcb = var = None
     if rank == 0 and world == 1 and not args.no_hamiltonian:
         ham = hamiltonian_bench(lap, a, b, phase, min(args.steps, 20))
         pcb = preconditioner_bench(gd, lap, a, b, phase, min(args.steps, 10))
+        var = stencil_variants_bench(gd, a, b, phase, min(args.steps, 20))
 
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic()
@@ -601,6 +655,8 @@ def run_gpu_arm(args):
         line['hamiltonian'] = ham
     if pcb is not None:
         line['preconditioner'] = pcb
+    if var is not None:
+        line['stencil_variants'] = var
     if rank == 0 and world == 1 and not args.no_poisson:
         try:
             pb, _, _, _ = poisson_bench()
