@@ -331,7 +331,7 @@ def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=300,
     return out
 
 
-def batch_bench():
+def batch_bench(transfer_bands=256):
     """32 simultaneous solves (8 each of 48, 64, 80, 96 points per axis, 16
     Gaussians, multicolour Gauss-Seidel) in one graph launch, and band-
     batched restriction/interpolation of 256 float64 bands 224^3 <-> 112^3
@@ -366,8 +366,9 @@ def batch_bench():
     fine = coarse.refine()
     g = torch.Generator(device='cuda')
     g.manual_seed(4)
-    c = torch.rand((256, 112, 112, 112), dtype=torch.float64, device='cuda', generator=g) * 2 - 1
-    f = torch.empty((256, 224, 224, 224), dtype=torch.float64, device='cuda')
+    nb = transfer_bands
+    c = torch.rand((nb, 112, 112, 112), dtype=torch.float64, device='cuda', generator=g) * 2 - 1
+    f = torch.empty((nb, 224, 224, 224), dtype=torch.float64, device='cuda')
     ip = Transformer(coarse, fine, 3)
     rs = Transformer(fine, coarse, 3)
     for _ in range(2):
@@ -380,10 +381,10 @@ def batch_bench():
     rs.apply(f, c)
     ev[2].record()
     torch.cuda.synchronize()
-    nfine = 256 * 224 ** 3
+    nfine = nb * 224 ** 3
     t_ip = ev[0].elapsed_time(ev[1]) * 1e-3
     t_rs = ev[1].elapsed_time(ev[2]) * 1e-3
-    out['transfers'] = {'workload': '256 float64 bands, 112^3 <-> 224^3, nn=3, periodic',
+    out['transfers'] = {'workload': '%d float64 bands, 112^3 <-> 224^3, nn=3, periodic' % nb,
                         'interpolate_GBps': 9 * nfine / t_ip / 1e9,
                         'restrict_GBps': 9 * nfine / t_rs / 1e9,
                         'interpolate_ms': t_ip * 1e3, 'restrict_ms': t_rs * 1e3}
@@ -702,6 +703,8 @@ def main():
     ap.add_argument('--requests', type=int, default=300, help='serving requests per rate')
     ap.add_argument('--no-serving', action='store_true')
     ap.add_argument('--no-hamiltonian', action='store_true')
+    ap.add_argument('--transfer-bands', type=int, default=256,
+                    help='bands of the transfer sub-benchmark (--only batch; smaller for profiling)')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference_arm(args)
@@ -714,7 +717,7 @@ def main():
         elif args.only == 'serving':
             print(json.dumps({'serving': serving_bench(nreq=args.requests)}))
         else:
-            print(json.dumps(batch_bench()))
+            print(json.dumps(batch_bench(args.transfer_bands)))
         return 0
     return run_gpu_arm(args)
 

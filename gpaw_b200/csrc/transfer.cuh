@@ -134,8 +134,12 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
   constexpr int CELLS = RY * RZ;
   constexpr int CC = (CELLS + NT - 1) / NT;
   constexpr int QL = 2 * W + 1;           // fine planes feeding one coarse plane
+  // Each staged fine row holds its even positions first, then its odd ones:
+  // the axis-2 taps of neighbouring coarse points are then consecutive
+  // words (a stride-2 read would hit every bank twice).
+  constexpr int HALF = (RZ + 1) / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZ]
+  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZ], rows de-interleaved
   V* T = F + 2 * CELLS;                           // [2][RY][BZC]
 
   const int t = threadIdx.x, tz = t % BZC, ty = t / BZC;
@@ -149,12 +153,15 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
   const int fy0 = 2 * Y0 - p.lo1, fz0 = 2 * Z0 - p.lo2;
 
   int src[CC];
+  int dpos[CC];  // stage position of cell t + i * NT
 #pragma unroll
   for (int i = 0; i < CC; i++) {
     int c = t + i * NT;
     src[i] = -1;
+    dpos[i] = 0;
     if (c < CELLS) {
       int sy = c / RZ, sz = c % RZ;
+      dpos[i] = sy * RZ + ((sz & 1) ? HALF + (sz >> 1) : (sz >> 1));
       int ysd, zsd;
       int ys = wrap_axis(fy0 + sy, p.ni1, p.per1, ysd);
       int zs = wrap_axis(fz0 + sz, p.ni2, p.per2, zsd);
@@ -192,14 +199,15 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
     V* Tb = T + (f & 1) * RY * BZC;
 #pragma unroll
     for (int i = 0; i < CC; i++)
-      if (t + i * NT < CELLS) Fb[t + i * NT] = rv[i];
+      if (t + i * NT < CELLS) Fb[dpos[i]] = rv[i];
     load(f + 1);
     __syncthreads();
-    // axis-2 pass: Tb[sy][cz] for every staged row
+    // axis-2 pass: Tb[sy][cz] for every staged row; fine position
+    // 2 cz + W + o sits at (W + o) & 1 ? HALF : 0, + cz + (W + o) / 2.
     for (int c = t; c < RY * BZC; c += NT) {
       const int sy = c / BZC, cz = c % BZC;
-      const V* row = Fb + sy * RZ + 2 * cz + W;
-      Tb[c] = rst_tap<NN, V>([&](int o) { return row[o]; });
+      const V* row = Fb + sy * RZ + cz;
+      Tb[c] = rst_tap<NN, V>([&](int o) { return row[((W + o) & 1 ? HALF : 0) + ((W + o) >> 1)]; });
     }
     __syncthreads();
     // axis-1 pass for this thread's coarse points, pushed into the queue
