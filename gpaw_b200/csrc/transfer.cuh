@@ -116,6 +116,23 @@ __device__ __forceinline__ V apply_phases(V v, int code, int xside, const Phases
   return v;
 }
 
+// Staged fine rows of the restriction kernel (RZ cells) are stored with
+// their even positions first and their odd ones from HALF on.  HALF sits
+// half a 128-byte segment past a segment start (E / 2 elements mod E), so
+// the even and odd runs that one shared-memory wavefront writes land in
+// different banks.
+template <class V, int RZ>
+constexpr int rst_half() {
+  constexpr int E = 128 / int(sizeof(V));
+  int h = (RZ + 1) / 2;
+  while (h % E != E / 2) ++h;
+  return h;
+}
+template <class V, int RZ>
+constexpr int rst_pitch() {
+  return rst_half<V, RZ>() + RZ / 2;
+}
+
 // ---------------------------------------------------------------------------
 // Restriction: coarse index i on an axis takes the fine padded point
 // (K-1) + 2i (c/bmgs/restrict.c:65-69), i.e. fine array index
@@ -137,10 +154,10 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
   // Each staged fine row holds its even positions first, then its odd ones:
   // the axis-2 taps of neighbouring coarse points are then consecutive
   // words (a stride-2 read would hit every bank twice).
-  constexpr int HALF = (RZ + 1) / 2;
+  constexpr int HALF = rst_half<V, RZ>(), RZP = rst_pitch<V, RZ>(), STG = RY * RZP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZ], rows de-interleaved
-  V* T = F + 2 * CELLS;                           // [2][RY][BZC]
+  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZP], rows de-interleaved
+  V* T = F + 2 * STG;                             // [2][RY][BZC]
 
   const int t = threadIdx.x, tz = t % BZC, ty = t / BZC;
   const int Z0 = blockIdx.x * BZC, Y0 = blockIdx.y * BYC;
@@ -161,7 +178,7 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
     dpos[i] = 0;
     if (c < CELLS) {
       int sy = c / RZ, sz = c % RZ;
-      dpos[i] = sy * RZ + ((sz & 1) ? HALF + (sz >> 1) : (sz >> 1));
+      dpos[i] = sy * RZP + ((sz & 1) ? HALF + (sz >> 1) : (sz >> 1));
       int ysd, zsd;
       int ys = wrap_axis(fy0 + sy, p.ni1, p.per1, ysd);
       int zs = wrap_axis(fz0 + sz, p.ni2, p.per2, zsd);
@@ -195,7 +212,7 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
 
   load(fbeg);
   for (int f = fbeg; f < fend; ++f) {
-    V* Fb = F + (f & 1) * CELLS;
+    V* Fb = F + (f & 1) * STG;
     V* Tb = T + (f & 1) * RY * BZC;
 #pragma unroll
     for (int i = 0; i < CC; i++)
@@ -206,7 +223,7 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
     // 2 cz + W + o sits at (W + o) & 1 ? HALF : 0, + cz + (W + o) / 2.
     for (int c = t; c < RY * BZC; c += NT) {
       const int sy = c / BZC, cz = c % BZC;
-      const V* row = Fb + sy * RZ + cz;
+      const V* row = Fb + sy * RZP + cz;
       Tb[c] = rst_tap<NN, V>([&](int o) { return row[((W + o) & 1 ? HALF : 0) + ((W + o) >> 1)]; });
     }
     __syncthreads();
