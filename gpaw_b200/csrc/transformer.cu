@@ -13,7 +13,9 @@ namespace gfd {
 template <class V, int NN>
 static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t nin,
                        TrParams<typename vt<V>::S>& p, cudaStream_t s) {
-  constexpr int BZC = 32, TYC = 8, VYC = 1, BYC = TYC * VYC;
+  // Two coarse rows per thread (16 per CTA) stage fewer halo rows per output
+  // row; complex128 keeps one, so two CTAs still fit on an SM.
+  constexpr int BZC = 32, TYC = 8, VYC = sizeof(V) >= 16 ? 1 : 2, BYC = TYC * VYC;
   constexpr int W = 2 * NN - 1;
   constexpr int RY = 2 * BYC - 1 + 2 * W, RZ = 2 * BZC - 1 + 2 * W;
   const size_t smem = (size_t)(2 * RY * rst_pitch<V, RZ>() + 2 * RY * BZC) * sizeof(V);
