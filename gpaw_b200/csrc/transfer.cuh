@@ -341,13 +341,20 @@ interp_kernel(const V* __restrict__ in, V* out, const V* base,
       if (t + i * NT < CELLS) Cb[t + i * NT] = rv[i];
     load(c + 1);
     __syncthreads();
-    // axis-2 pass: every staged coarse row to this tile's fine columns
-    for (int e = t; e < CY * BZF; e += NT) {
-      const int sy = e / BZF, fz = e % BZF;
+    // axis-2 pass: every staged coarse row to this tile's fine columns, two
+    // adjacent fine columns per thread (one even, one odd, whatever the
+    // skip), so every lane does one copy and one K-tap value.
+    static_assert(BZF % 2 == 0, "fine columns come in pairs");
+    for (int e = t; e < CY * (BZF / 2); e += NT) {
+      const int sy = e / (BZF / 2), fz = 2 * (e % (BZF / 2));
       const int g = Z0 + fz + p.sk2;
-      const int cl = (g >> 1) - iz0 + NN - 1;
-      const V* row = Cb + sy * CZ + cl;
-      Tb[e] = (g & 1) ? ip_tap<NN, V>([&](int o) { return row[o]; }) : row[0];
+      const int odd0 = g & 1;  // the same for every pair of the tile
+      const int ge = g + odd0, go = g + 1 - odd0;  // the pair's even and odd g
+      const V* rowe = Cb + sy * CZ + ((ge >> 1) - iz0 + NN - 1);
+      const V* rowo = Cb + sy * CZ + ((go >> 1) - iz0 + NN - 1);
+      V* out = Tb + sy * BZF + fz;
+      out[odd0] = rowe[0];
+      out[1 - odd0] = ip_tap<NN, V>([&](int o) { return rowo[o]; });
     }
     __syncthreads();
     // axis-1 pass for this thread's fine points
