@@ -31,10 +31,13 @@ int check_cuda(cudaError_t e, const char* what) {
 
 int check_launch(const char* what) { return check_cuda(cudaGetLastError(), what); }
 
+// Programmatic dependent launch is opt-in (GFD_PDL=1): in the Poisson solve
+// graph, whose kernels are short, starting dependents early cost 3% of
+// solves/s; the streaming kernels neither gain nor lose.
 bool pdl_enabled() {
   static const bool on = [] {
     const char* e = getenv("GFD_PDL");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return on;
 }

@@ -151,8 +151,8 @@ long long direct_max_points();
 // chunks (GFD_MARCH_CTAS_PER_SM, default 4).
 int march_ctas_per_sm();
 
-// Launch with the programmatic-stream-serialisation attribute (when
-// enabled; GFD_PDL=0 in the environment turns it off).
+// Launch with the programmatic-stream-serialisation attribute when enabled
+// (GFD_PDL=1 in the environment; off by default).
 template <class... P, class... A>
 inline cudaError_t launch_k(void (*kern)(P...), dim3 grid, dim3 block, size_t smem,
                             cudaStream_t s, A&&... args) {
