@@ -332,15 +332,19 @@ interp_kernel(const V* __restrict__ in, V* out, const V* base,
 #pragma unroll
     for (int k = 0; k < QL; k++) q[j][k] = vzero<V>();
 
+  // One barrier per coarse plane: plane c + 1 is staged (into the other
+  // buffer) while plane c's axis-2 results are being written, and both C
+  // and T are double-buffered, so every read of a buffer is separated from
+  // the next write into it by a barrier.
   load(cbeg);
-  for (int c = cbeg; c < cend; ++c) {
-    V* Cb = C + (c & 1) * CELLS;
-    V* Tb = T + (c & 1) * CY * BZF;
 #pragma unroll
-    for (int i = 0; i < CC; i++)
-      if (t + i * NT < CELLS) Cb[t + i * NT] = rv[i];
-    load(c + 1);
-    __syncthreads();
+  for (int i = 0; i < CC; i++)
+    if (t + i * NT < CELLS) C[(cbeg & 1) * CELLS + t + i * NT] = rv[i];
+  load(cbeg + 1);
+  __syncthreads();
+  for (int c = cbeg; c < cend; ++c) {
+    const V* Cb = C + (c & 1) * CELLS;
+    V* Tb = T + (c & 1) * CY * BZF;
     // axis-2 pass: every staged coarse row to this tile's fine columns, two
     // adjacent fine columns per thread (one even, one odd, whatever the
     // skip), so every lane does one copy and one K-tap value.
@@ -355,6 +359,13 @@ interp_kernel(const V* __restrict__ in, V* out, const V* base,
       V* out = Tb + sy * BZF + fz;
       out[odd0] = rowe[0];
       out[1 - odd0] = ip_tap<NN, V>([&](int o) { return rowo[o]; });
+    }
+    if (c + 1 < cend) {
+      V* Cn = C + ((c + 1) & 1) * CELLS;
+#pragma unroll
+      for (int i = 0; i < CC; i++)
+        if (t + i * NT < CELLS) Cn[t + i * NT] = rv[i];
+      load(c + 2);
     }
     __syncthreads();
     // axis-1 pass for this thread's fine points
