@@ -258,7 +258,7 @@ def poisson_rho(gd, ng, seed):
     return rho - rho.mean()
 
 
-def poisson_bench(nsolves=8):
+def poisson_bench(nsolves=8, tune=True):
     import torch
     from gpaw_b200.grid_descriptor import GridDescriptor
     from gpaw_b200.poisson import PoissonSolver
@@ -272,6 +272,8 @@ def poisson_bench(nsolves=8):
         ps = PoissonSolver(3, 'J', 2e-10, precision=prec)
         ps.set_grid_descriptor(gd)
         ps.initialize()
+        if tune:
+            ps.autotune(reps=5)
         phi = torch.zeros_like(rho)
         ps.solve(phi, rho)  # warm-up
         lat = []
@@ -286,7 +288,7 @@ def poisson_bench(nsolves=8):
         lat = np.array(lat)
         out[prec] = {'solves_per_s': float(1.0 / lat.mean()), 'p50_ms': float(np.median(lat) * 1e3),
                      'p99_ms': float(np.percentile(lat, 99) * 1e3), 'vcycles': int(niter),
-                     'residual': float(ps.error)}
+                     'residual': float(ps.error), 'autotuned': bool(tune)}
     out['mixed_vs_fp64_speedup'] = out['mixed']['solves_per_s'] / out['fp64']['solves_per_s']
     out['mixed_max_abs_vs_fp64'] = float(np.abs(phis['mixed'] - phis['fp64']).max())
     return out, phis, rho_h, gd
@@ -331,12 +333,14 @@ def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=300,
     return out
 
 
-def batch_bench(transfer_bands=256):
+def batch_bench(transfer_bands=256, tune=True):
     """32 simultaneous solves (8 each of 48, 64, 80, 96 points per axis, 16
     Gaussians, multicolour Gauss-Seidel) in one graph launch, and band-
     batched restriction/interpolation of 256 float64 bands 224^3 <-> 112^3
-    (nn=3, periodic)."""
+    (nn=3, periodic).  tune: autotune the launch plans first (one solver per
+    grid size; the others share its plans through the cache)."""
     import torch
+    from gpaw_b200 import autotune
     from gpaw_b200.poisson import PoissonSolver
     from gpaw_b200.serving import PoissonBatch, grid_for
     from gpaw_b200.transformers import Transformer
@@ -348,10 +352,12 @@ def batch_bench(transfer_bands=256):
         ps = PoissonSolver(3, 'GS', 2e-10)
         ps.set_grid_descriptor(gd)
         ps.initialize()
+        if tune and i % 8 == 0:
+            ps.autotune(reps=3)
         solvers.append(ps)
         rhos.append(torch.from_numpy(poisson_rho(gd, 16, 40 + i)).cuda())
         phis.append(torch.zeros_like(rhos[-1]))
-    batch = PoissonBatch(solvers)
+    batch = PoissonBatch(solvers)  # captured with the tuned plans
     batch.solve(phis, rhos)  # warm-up (captures the graph)
     for p in phis:
         p.zero_()
@@ -361,7 +367,8 @@ def batch_bench(transfer_bands=256):
     dt = time.perf_counter() - t0
     out = {'poisson_batch': {'workload': '32 solves, 8 each of 48,64,80,96^3, GS, one launch',
                              'seconds': dt, 'solves_per_s': 32 / dt,
-                             'vcycles': [r[0] for r in res], 'max_residual': max(r[1] for r in res)}}
+                             'vcycles': [r[0] for r in res], 'max_residual': max(r[1] for r in res),
+                             'autotuned': bool(tune)}}
     coarse = GridDescriptor((112,) * 3, (112 * 0.3,) * 3, 1)
     fine = coarse.refine()
     g = torch.Generator(device='cuda')
@@ -371,6 +378,10 @@ def batch_bench(transfer_bands=256):
     f = torch.empty((nb, 224, 224, 224), dtype=torch.float64, device='cuda')
     ip = Transformer(coarse, fine, 3)
     rs = Transformer(fine, coarse, 3)
+    plans = None
+    if tune:
+        plans = {'interpolate': autotune.tune_transformer(ip, nb, reps=2),
+                 'restrict': autotune.tune_transformer(rs, nb, reps=2)}
     for _ in range(2):
         ip.apply(c, f)
         rs.apply(f, c)
@@ -387,7 +398,8 @@ def batch_bench(transfer_bands=256):
     out['transfers'] = {'workload': '%d float64 bands, 112^3 <-> 224^3, nn=3, periodic' % nb,
                         'interpolate_GBps': 9 * nfine / t_ip / 1e9,
                         'restrict_GBps': 9 * nfine / t_rs / 1e9,
-                        'interpolate_ms': t_ip * 1e3, 'restrict_ms': t_rs * 1e3}
+                        'interpolate_ms': t_ip * 1e3, 'restrict_ms': t_rs * 1e3,
+                        'launch_plans': plans}
     del c, f
     return out
 
@@ -575,6 +587,10 @@ def run_gpu_arm(args):
     b = torch.empty_like(a)
     stream = torch.cuda.current_stream()
     nbytes = BYTES_PER_POINT * nb * N ** 3
+    plan = None
+    if not args.no_autotune:
+        from gpaw_b200 import autotune
+        plan = autotune.tune_operator(lap, nb, phase_cd=phase, reps=3)
 
     for _ in range(args.warmup):
         lap.apply(a, b, phase)
@@ -648,7 +664,10 @@ def run_gpu_arm(args):
             'roofline': {'bound': 'hbm', 'achieved': kernel_gbs, 'peak': peak, 'unit': 'GB/s',
                          'frac': kernel_gbs / peak, 'peak_kind': peak_kind,
                          'traffic': traffic, 'algorithmic_bytes_per_launch': nbytes,
-                         'kernel': 'star_kernel<cplx<double>,R=3>'},
+                         'kernel': ('star_direct_kernel<cplx<double>,R=3>'
+                                    if plan and plan['form'] == 'direct'
+                                    else 'star_kernel<cplx<double>,R=3>')},
+            'launch_plan': plan,
             'e2e': e2e,
             'gpu_launches': args.steps,
             'clocks': clocks.result()}
@@ -660,14 +679,14 @@ def run_gpu_arm(args):
         line['stencil_variants'] = var
     if rank == 0 and world == 1 and not args.no_poisson:
         try:
-            pb, _, _, _ = poisson_bench()
+            pb, _, _, _ = poisson_bench(tune=not args.no_autotune)
             line['poisson'] = pb
         except Exception as e:  # reported, never hidden
             line['poisson'] = {'error': repr(e)}
     if rank == 0 and world == 1 and not args.no_poisson and not args.no_serving:
         try:
             line['serving'] = serving_bench(nreq=args.requests)
-            line.update(batch_bench())
+            line.update(batch_bench(tune=not args.no_autotune))
         except Exception as e:  # reported, never hidden
             line['serving'] = {'error': repr(e)}
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -703,6 +722,8 @@ def main():
     ap.add_argument('--requests', type=int, default=300, help='serving requests per rate')
     ap.add_argument('--no-serving', action='store_true')
     ap.add_argument('--no-hamiltonian', action='store_true')
+    ap.add_argument('--no-autotune', action='store_true',
+                    help='keep the built-in launch rules (no plan tuning before timing)')
     ap.add_argument('--transfer-bands', type=int, default=256,
                     help='bands of the transfer sub-benchmark (--only batch; smaller for profiling)')
     args = ap.parse_args()
@@ -712,12 +733,12 @@ def main():
         import torch
         torch.cuda.set_device(0)
         if args.only == 'poisson':
-            pb, _, _, _ = poisson_bench(args.solves)
+            pb, _, _, _ = poisson_bench(args.solves, not args.no_autotune)
             print(json.dumps({'poisson': pb}))
         elif args.only == 'serving':
             print(json.dumps({'serving': serving_bench(nreq=args.requests)}))
         else:
-            print(json.dumps(batch_bench(args.transfer_bands)))
+            print(json.dumps(batch_bench(args.transfer_bands, not args.no_autotune)))
         return 0
     return run_gpu_arm(args)
 

@@ -33,6 +33,22 @@ GFD_RELAX_JACOBI = 2
 GFD_POISSON_FP64 = 0
 GFD_POISSON_MIXED = 1
 
+GFD_TUNE_APPLY = 0
+GFD_TUNE_JACOBI = 1
+GFD_TUNE_POTENTIAL = 3
+
+
+class TunePlan(ctypes.Structure):
+    """gfd_tune_plan: form 0 one thread per point / 1 marching kernel, the
+    marching tile (0: 32 columns, 1: 16, 2: 8), the axis-0 split target in
+    CTAs per SM and the measured microseconds per launch."""
+    _fields_ = [('form', ctypes.c_int), ('tile', ctypes.c_int), ('ctas_per_sm', ctypes.c_int),
+                ('us', ctypes.c_double)]
+
+    def as_dict(self):
+        return {'form': ('direct', 'march')[self.form], 'tile': (32, 16, 8)[self.tile],
+                'ctas_per_sm': self.ctas_per_sm, 'us': self.us}
+
 # Every function the header declares: name -> (restype, argtypes).
 _vp = ctypes.c_void_p
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -83,6 +99,20 @@ SIGNATURES = {
                                                      ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                      _vp]),
     'gfd_grid_sum': (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double, _dp, _vp]),
+    'gfd_autotune_operator': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp,
+                                             ctypes.c_int64, _dp, ctypes.c_double, ctypes.c_int,
+                                             _vp, ctypes.POINTER(TunePlan)]),
+    'gfd_autotune_transformer': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int64,
+                                                ctypes.c_int, _vp, ctypes.POINTER(TunePlan)]),
+    'gfd_autotune_operator_plan': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                                  ctypes.POINTER(TunePlan), _ip]),
+    'gfd_autotune_transformer_plan': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64,
+                                                     ctypes.POINTER(TunePlan), _ip]),
+    'gfd_autotune_count': (ctypes.c_int, [_ip]),
+    'gfd_autotune_clear': (ctypes.c_int, []),
+    'gfd_autotune_save': (ctypes.c_int, [ctypes.c_char_p]),
+    'gfd_autotune_load': (ctypes.c_int, [ctypes.c_char_p]),
+    'gfd_poisson_autotune': (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
 }
 
 

@@ -177,6 +177,11 @@ int check_cuda(cudaError_t e, const char* what);
 int check_launch(const char* what);
 
 inline int dtype_is_complex(int dtype) { return dtype == GFD_COMPLEX128 || dtype == GFD_COMPLEX64; }
+template <class V>
+constexpr int dtype_of() {
+  return vt<V>::NC == 2 ? (sizeof(typename vt<V>::S) == 8 ? GFD_COMPLEX128 : GFD_COMPLEX64)
+                        : (sizeof(typename vt<V>::S) == 8 ? GFD_FLOAT64 : GFD_FLOAT32);
+}
 inline int dtype_is_fp32(int dtype) { return dtype == GFD_FLOAT32 || dtype == GFD_COMPLEX64; }
 inline size_t dtype_size(int dtype) {
   switch (dtype) {

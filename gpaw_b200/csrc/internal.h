@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <tuple>
 #include <vector>
 
 #include "gpaw_fd.h"
@@ -46,6 +47,38 @@ namespace gfd {
 enum { OP_APPLY = 0, OP_JACOBI = 1, OP_RESIDUAL = 2, OP_POTENTIAL = 3, OP_JACOBI_NEG = 4 };
 
 int num_sms();
+
+// ---------------------------------------------------------------------------
+// Launch plans (autotune.cu).  A plan fixes, for one kernel family, element
+// type, mode, grid, stencil radius (or transfer order), boundary conditions
+// and band-count class, the kernel form and the axis-0 split.  Launches use
+// the cached plan when there is one and the built-in rules otherwise.
+// ---------------------------------------------------------------------------
+enum { TILE_WIDE = 0, TILE_MID = 1, TILE_NARROW = 2 };  // marching tiles 32 / 16 / 8 wide
+enum { PLAN_DIRECT = 0, PLAN_MARCH = 1 };               // one thread per point / marching
+enum { TK_STAR = 0, TK_RESTRICT = 1, TK_INTERP = 2 };
+
+struct TuneKey {
+  int kind, dtype, mode, n0, n1, n2, order, per, nbc;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(kind, dtype, mode, n0, n1, n2, order, per, nbc) <
+           std::tie(o.kind, o.dtype, o.mode, o.n0, o.n1, o.n2, o.order, o.per, o.nbc);
+  }
+};
+struct TunePlan {
+  int path = PLAN_MARCH;
+  int tile = TILE_WIDE;
+  int cps = 4;       // target CTAs per SM of the axis-0 split
+  double us = 0.0;   // measured time per launch
+};
+// Star operator launch of nin bands in mode OP_APPLY / OP_JACOBI(_NEG) /
+// OP_POTENTIAL (residual sweeps keep the built-in rules: the Poisson solver
+// sizes its partial-sum buffer from them).
+TuneKey star_tune_key(const gfd_operator* op, int dtype, int mode, int64_t nin);
+TuneKey tr_tune_key(const gfd_transformer* tr, int dtype, int64_t nin);
+// The plan of an autotune run in progress on this thread, else the cached
+// one; false: no plan, use the built-in rules.
+bool tune_lookup(const TuneKey& k, TunePlan* plan);
 
 // Stencil launch.  mode OP_APPLY: out = L in.  OP_JACOBI: out = Jacobi update
 // of in with source rho and weight w.  OP_RESIDUAL: out = L in - rho and, if

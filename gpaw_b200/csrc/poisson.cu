@@ -622,6 +622,13 @@ extern "C" int gfd_poisson_destroy(gfd_poisson* ps) {
   return GFD_OK;
 }
 
+static void drop_graph(gfd_poisson* ps) {
+  if (ps->exec) cudaGraphExecDestroy(ps->exec);
+  if (ps->graph) cudaGraphDestroy(ps->graph);
+  ps->exec = nullptr;
+  ps->graph = nullptr;
+}
+
 extern "C" int gfd_poisson_set_rhs_operator(gfd_poisson* ps, gfd_operator* B) {
   if (!ps) return set_error(GFD_EINVAL, "null solver");
   if (B) {
@@ -632,10 +639,33 @@ extern "C" int gfd_poisson_set_rhs_operator(gfd_poisson* ps, gfd_operator* B) {
   }
   ps->B = B;
   // The solve graph holds the old prologue: capture it again on the next solve.
-  if (ps->exec) cudaGraphExecDestroy(ps->exec);
-  if (ps->graph) cudaGraphDestroy(ps->graph);
-  ps->exec = nullptr;
-  ps->graph = nullptr;
+  drop_graph(ps);
+  return GFD_OK;
+}
+
+extern "C" int gfd_poisson_autotune(gfd_poisson* ps, int reps, void* stream) {
+  if (!ps) return set_error(GFD_EINVAL, "null solver");
+  gfd_tune_plan plan;
+  int st;
+  // The level buffers are scratch between solves: the timed launches may
+  // overwrite them.
+  for (int l = 0; l <= ps->levels; l++) {
+    Level& lv = ps->L[l];
+    if (ps->relax_method != GFD_RELAX_GS && lv.op->star && lv.w != 0.0 &&
+        (st = gfd_autotune_operator(lv.op, ps->vdtype, GFD_TUNE_JACOBI, lv.phi[0], lv.phi[1],
+                                    lv.rho, 1, nullptr, lv.w, reps, stream, &plan)))
+      return st;
+    if (l < ps->levels) {
+      Level& nx = ps->L[l + 1];
+      if ((st = gfd_autotune_transformer(ps->restr[l], ps->vdtype, lv.res, nx.rho, 1, reps, stream,
+                                         &plan)))
+        return st;
+      if ((st = gfd_autotune_transformer(ps->interp[l], ps->vdtype, nx.phi[0], lv.res, 1, reps,
+                                         stream, &plan)))
+        return st;
+    }
+  }
+  drop_graph(ps);
   return GFD_OK;
 }
 

@@ -12,10 +12,9 @@
 
 namespace gfd {
 
-// Tile shapes (BZ x TY threads, VY rows per thread, D planes of prefetch).
+// Tile shapes (BZ x TY threads, VY rows per thread; TILE_* in internal.h).
 // Wide tiles for grids whose fastest axis fills a warp, narrow ones for the
 // small coarse multigrid levels.
-enum { TILE_WIDE = 0, TILE_MID = 1, TILE_NARROW = 2 };
 
 inline int pick_tile(const gfd_operator* op) {
   if (op->R > 2) return TILE_WIDE;
@@ -63,13 +62,14 @@ struct LaunchGeom {
   int64_t bands_per_launch;
 };
 
-inline LaunchGeom star_geom(const gfd_operator* op, int tile, int64_t nin, int R) {
+inline LaunchGeom star_geom(const gfd_operator* op, int tile, int64_t nin, int R,
+                            int cps = 0) {
   TileDims td = tile_dims(tile);
   LaunchGeom g;
   int gx = (op->n[2] + td.BZ - 1) / td.BZ;
   int gy = (op->n[1] + td.BY - 1) / td.BY;
   int64_t tiles = (int64_t)gx * gy * std::max<int64_t>(nin, 1);
-  int64_t target = (int64_t)march_ctas_per_sm() * num_sms();
+  int64_t target = (int64_t)(cps > 0 ? cps : march_ctas_per_sm()) * num_sms();
   int maxc = std::max(1, op->n[0] / std::max(4, 2 * R));
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   g.x_chunk = (op->n[0] + nxc - 1) / nxc;
@@ -285,7 +285,10 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
       return set_error(GFD_EUNSUPPORTED, "complex Jacobi/residual sweeps need radius <= 3");
   }
   if (mode == OP_POTENTIAL) p.pot = rho;  // the potential travels as the source argument
-  if (use_direct(op, nin)) {
+  TunePlan plan;
+  const bool tuned =
+      mode != OP_RESIDUAL && tune_lookup(star_tune_key(op, dtype_of<V>(), mode, nin), &plan);
+  if (tuned ? plan.path == PLAN_DIRECT : use_direct(op, nin)) {
     p.partials = partials;
     const long long total = (long long)p.band * nin;
     if (mode == OP_POTENTIAL)
@@ -297,15 +300,16 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
     return direct_dispatch<V, MODE_APPLY>(op, vin, vout, nullptr, p, total, s);
   }
   if constexpr (std::is_same_v<V, cplx<double>>) {
-    if (mode == OP_APPLY && tma_eligible(op, in)) {
+    if (!tuned && mode == OP_APPLY && tma_eligible(op, in)) {
       LaunchGeom g = star_geom(op, TILE_WIDE, nin, op->R);
       p.nxc = g.nxc;
       p.x_chunk = g.x_chunk;
       return star_tma_dispatch(op, vin, vout, nin, p, g, s);
     }
   }
-  const int tile = pick_tile(op);
-  LaunchGeom g = star_geom(op, tile, nin, op->R);
+  // Radii above 2 have the wide tile only.
+  const int tile = tuned && op->R <= 2 ? plan.tile : pick_tile(op);
+  LaunchGeom g = star_geom(op, tile, nin, op->R, tuned ? plan.cps : 0);
   p.nxc = g.nxc;
   p.x_chunk = g.x_chunk;
   if (mode == OP_POTENTIAL)

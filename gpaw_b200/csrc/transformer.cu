@@ -12,7 +12,7 @@ namespace gfd {
 
 template <class V, int NN>
 static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t nin,
-                       TrParams<typename vt<V>::S>& p, cudaStream_t s) {
+                       TrParams<typename vt<V>::S>& p, int cps, cudaStream_t s) {
   // Two coarse rows per thread (16 per CTA) stage fewer halo rows per output
   // row; complex128 keeps one, so two CTAs still fit on an SM.
   constexpr int BZC = 32, TYC = 8, VYC = sizeof(V) >= 16 ? 1 : 2, BYC = TYC * VYC;
@@ -21,7 +21,7 @@ static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t n
   const size_t smem = (size_t)(2 * RY * rst_pitch<V, RZ>() + 2 * RY * BZC) * sizeof(V);
   const int gx = (tr->nout[2] + BZC - 1) / BZC, gy = (tr->nout[1] + BYC - 1) / BYC;
   const int64_t tiles = (int64_t)gx * gy * nin;
-  const int64_t target = (int64_t)march_ctas_per_sm() * num_sms();
+  const int64_t target = (int64_t)(cps > 0 ? cps : march_ctas_per_sm()) * num_sms();
   int maxc = std::max(1, tr->nout[0] / 2);
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   p.x_chunk = (tr->nout[0] + nxc - 1) / nxc;
@@ -40,13 +40,13 @@ static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t n
 
 template <class V, int NN>
 static int interp_go(const gfd_transformer* tr, const V* in, V* out, const V* base, int64_t nin,
-                     TrParams<typename vt<V>::S>& p, cudaStream_t s) {
+                     TrParams<typename vt<V>::S>& p, int cps, cudaStream_t s) {
   constexpr int BZF = 64, TYF = 4, VYF = 2, BYF = TYF * VYF;
   constexpr int CY = BYF / 2 + 2 * NN, CZ = BZF / 2 + 2 * NN;
   const size_t smem = (size_t)(2 * CY * CZ + 2 * CY * BZF) * sizeof(V);
   const int gx = (tr->nout[2] + BZF - 1) / BZF, gy = (tr->nout[1] + BYF - 1) / BYF;
   const int64_t tiles = (int64_t)gx * gy * nin;
-  const int64_t target = (int64_t)march_ctas_per_sm() * num_sms();
+  const int64_t target = (int64_t)(cps > 0 ? cps : march_ctas_per_sm()) * num_sms();
   int maxc = std::max(1, tr->nout[0] / 4);
   int nxc = (int)std::min<int64_t>(maxc, std::max<int64_t>(1, (target + tiles - 1) / tiles));
   p.x_chunk = (tr->nout[0] + nxc - 1) / nxc;
@@ -95,7 +95,10 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const 
   const V* base = static_cast<const V*>(base_v);
   if (base && !tr->interpolate)
     return set_error(GFD_EINVAL, "subtracting form is for interpolation only");
-  if (p.band_out * nin <= direct_max_points()) {
+  TunePlan plan;
+  const bool tuned = tune_lookup(tr_tune_key(tr, dtype_of<V>(), nin), &plan);
+  const int cps = tuned ? plan.cps : 0;
+  if (tuned ? plan.path == PLAN_DIRECT : p.band_out * nin <= direct_max_points()) {
     switch (tr->nn) {
       case 1: return direct_go<V, 1>(tr, vin, vout, base, nin, p, s);
       case 2: return direct_go<V, 2>(tr, vin, vout, base, nin, p, s);
@@ -105,18 +108,18 @@ static int tr_typed(const gfd_transformer* tr, const void* in, void* out, const 
   }
   if (tr->interpolate) {
     switch (tr->nn) {
-      case 1: return interp_go<V, 1>(tr, vin, vout, base, nin, p, s);
-      case 2: return interp_go<V, 2>(tr, vin, vout, base, nin, p, s);
-      case 3: return interp_go<V, 3>(tr, vin, vout, base, nin, p, s);
-      case 4: return interp_go<V, 4>(tr, vin, vout, base, nin, p, s);
+      case 1: return interp_go<V, 1>(tr, vin, vout, base, nin, p, cps, s);
+      case 2: return interp_go<V, 2>(tr, vin, vout, base, nin, p, cps, s);
+      case 3: return interp_go<V, 3>(tr, vin, vout, base, nin, p, cps, s);
+      case 4: return interp_go<V, 4>(tr, vin, vout, base, nin, p, cps, s);
     }
   } else {
     if (base) return set_error(GFD_EINVAL, "subtracting form is for interpolation only");
     switch (tr->nn) {
-      case 1: return restrict_go<V, 1>(tr, vin, vout, nin, p, s);
-      case 2: return restrict_go<V, 2>(tr, vin, vout, nin, p, s);
-      case 3: return restrict_go<V, 3>(tr, vin, vout, nin, p, s);
-      case 4: return restrict_go<V, 4>(tr, vin, vout, nin, p, s);
+      case 1: return restrict_go<V, 1>(tr, vin, vout, nin, p, cps, s);
+      case 2: return restrict_go<V, 2>(tr, vin, vout, nin, p, cps, s);
+      case 3: return restrict_go<V, 3>(tr, vin, vout, nin, p, cps, s);
+      case 4: return restrict_go<V, 4>(tr, vin, vout, nin, p, cps, s);
     }
   }
   return set_error(GFD_EINVAL, "k must be 2, 4, 6 or 8");

@@ -152,6 +152,18 @@ class PoissonSolver:
                         device=self.gd.device)
         self.solve(z, torch.zeros_like(z))
 
+    def autotune(self, reps=5):
+        """Tune the launch plans of every level's Jacobi sweep, restriction
+        and interpolation on the solver's own buffers
+        (gpaw_b200.autotune); the next solve captures its graph with them."""
+        import torch
+        if self.solver is None:
+            self.initialize()
+        _lib.check(_lib.lib.gfd_poisson_autotune(
+            self.solver, int(reps), torch.cuda.current_stream(self.gd.device).cuda_stream),
+            'PoissonSolver.autotune')
+        torch.cuda.current_stream(self.gd.device).synchronize()
+
     def solve_async(self, phi, rho, charge=None, eps=None, maxcharge=1e-6):
         """Enqueue a solve on the current stream and return at once; call
         result() after the stream has passed it (e.g. a recorded event)."""

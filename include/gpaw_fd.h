@@ -276,6 +276,60 @@ GFD_API int gfd_poisson_batch_solve_async(gfd_poisson_batch* batch, double* cons
                                           int maxiter, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Launch-plan autotuning.  No counterpart in the reference, whose CPU code
+ * has one path per operation; it serves the same call sites (Operator.apply
+ * and relax, c/operators.c:316-405 and :49-91; Transformer.apply,
+ * c/transformers.c:127-185) by choosing how they run on the GPU.
+ *
+ * A plan fixes the kernel form (one thread per point, or the marching
+ * kernel that streams planes along axis 0), the marching tile and the
+ * axis-0 split (target CTAs per SM, i.e. the planes each CTA marches
+ * through).  gfd_autotune_operator / _transformer time every candidate with
+ * CUDA events on the caller's buffers and stream (reps timed launches each,
+ * after one untimed launch; the output buffer is overwritten) and cache the
+ * fastest under (operation, dtype, mode, grid, radius or order, boundary
+ * conditions, floor(log2(bands))).  Later launches with that key use it;
+ * others keep the built-in rules.  Marching candidates give bit-identical
+ * results; the one-thread-per-point form sums a stencil's terms in another
+ * order (rounding-level differences).  Residual sweeps keep the built-in
+ * rules.  Not allowed on a stream that is being captured.
+ * Plans take effect at the next launch: a Poisson solver's or batch's
+ * captured graph keeps the plans it was captured with
+ * (gfd_poisson_autotune recaptures).  GFD_TUNE_CACHE=<path> loads a saved
+ * cache on first use.
+ * ---------------------------------------------------------------------- */
+#define GFD_TUNE_APPLY 0      /* gfd_operator_apply */
+#define GFD_TUNE_JACOBI 1     /* one weighted-Jacobi sweep (src = rho, weight w) */
+#define GFD_TUNE_POTENTIAL 3  /* gfd_operator_apply_potential (src = v) */
+
+typedef struct gfd_tune_plan {
+  int form;         /* 0: one thread per point; 1: marching kernel */
+  int tile;         /* marching tile: 0 32 columns, 1 16, 2 8 */
+  int ctas_per_sm;  /* axis-0 split target */
+  double us;        /* measured time per launch, microseconds */
+} gfd_tune_plan;
+
+GFD_API int gfd_autotune_operator(gfd_operator* op, int dtype, int mode, const void* in, void* out,
+                                  const void* src, int64_t nin, const double* phase_cd, double w,
+                                  int reps, void* stream, gfd_tune_plan* best);
+GFD_API int gfd_autotune_transformer(gfd_transformer* tr, int dtype, const void* in, void* out,
+                                     int64_t nin, int reps, void* stream, gfd_tune_plan* best);
+/* The cached plan for a launch: *found = 1 and *plan filled, or *found = 0. */
+GFD_API int gfd_autotune_operator_plan(const gfd_operator* op, int dtype, int mode, int64_t nin,
+                                       gfd_tune_plan* plan, int* found);
+GFD_API int gfd_autotune_transformer_plan(const gfd_transformer* tr, int dtype, int64_t nin,
+                                          gfd_tune_plan* plan, int* found);
+GFD_API int gfd_autotune_count(int* n);
+GFD_API int gfd_autotune_clear(void);
+/* Text file, one plan per line; load merges into the cache. */
+GFD_API int gfd_autotune_save(const char* path);
+GFD_API int gfd_autotune_load(const char* path);
+/* Tune every level's Jacobi sweep and every restriction and interpolation of
+ * a solver on its own level buffers, then drop its captured graph so the next
+ * solve uses the plans.  Batches capture at creation: tune first. */
+GFD_API int gfd_poisson_autotune(gfd_poisson* ps, int reps, void* stream);
+
+/* ------------------------------------------------------------------------
  * Reductions.
  * sum over all points of a float64 array of n elements, times scale (the
  * integral of GridDescriptor.integrate, gpaw/grid_descriptor.py:197-215).

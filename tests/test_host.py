@@ -162,3 +162,48 @@ def test_no_cpu_path_for_host_tensors():
     a = torch.zeros((8, 8, 8), dtype=torch.float64)
     with pytest.raises(ValueError, match='CUDA'):
         op.apply(a, torch.zeros_like(a))
+
+
+def test_tune_cache_file_roundtrip(tmp_path):
+    """The launch-plan cache loads, counts, saves, rejects malformed files and
+    clears without touching a GPU; plans are looked up by operator key."""
+    from gpaw_b200 import _lib
+    lib = _lib.lib
+    n = ctypes.c_int(-1)
+    assert lib.gfd_autotune_clear() == 0
+    good = tmp_path / 'plans.txt'
+    good.write_text('gfd-tune 1\n# comment\n'
+                    '0 1 0 96 96 96 3 7 9 1 0 2 1234.5\n'
+                    '1 0 0 224 224 224 3 7 8 0 0 4 99.0\n')
+    assert lib.gfd_autotune_load(str(good).encode()) == 0
+    assert lib.gfd_autotune_count(ctypes.byref(n)) == 0 and n.value == 2
+    st, h = _create_op([-3.0, 1, 1, 0.5, 0.5, 0.25, 0.25, 0.1, 0.1, 0.05, 0.05, 0.02, 0.02,
+                        0.01, 0.01, 0.005, 0.005, 0.001, 0.001],
+                       [(0, 0, 0)] + [tuple(s * k * e for e in np.eye(3, dtype=int)[a])
+                                      for k in (1, 2, 3) for a in range(3) for s in (1, -1)],
+                       (96, 96, 96), nbr=[0] * 6, real=0)
+    assert st == 0
+    plan = _lib.TunePlan()
+    found = ctypes.c_int(0)
+    assert lib.gfd_autotune_operator_plan(h, _lib.GFD_COMPLEX128, _lib.GFD_TUNE_APPLY, 512,
+                                          ctypes.byref(plan), ctypes.byref(found)) == 0
+    assert found.value == 1 and plan.as_dict() == {'form': 'march', 'tile': 32,
+                                                   'ctas_per_sm': 2, 'us': 1234.5}
+    assert lib.gfd_autotune_operator_plan(h, _lib.GFD_COMPLEX128, _lib.GFD_TUNE_APPLY, 256,
+                                          ctypes.byref(plan), ctypes.byref(found)) == 0
+    assert found.value == 0   # another band-count class
+    lib.gfd_operator_destroy(h)
+    out = tmp_path / 'saved.txt'
+    assert lib.gfd_autotune_save(str(out).encode()) == 0
+    lines = [ln.split() for ln in out.read_text().splitlines()[1:] if not ln.startswith('#')]
+    assert sorted(tuple(map(float, ln)) for ln in lines) == sorted([
+        (0, 1, 0, 96, 96, 96, 3, 7, 9, 1, 0, 2, 1234.5), (1, 0, 0, 224, 224, 224, 3, 7, 8, 0, 0, 4, 99.0)])
+    for bad in ('not a cache\n', 'gfd-tune 1\n0 1 0 96 96 96 3 7 9 5 0 2 1.0\n',
+                'gfd-tune 1\n0 1 0 96\n'):
+        p = tmp_path / 'bad.txt'
+        p.write_text(bad)
+        assert lib.gfd_autotune_load(str(p).encode()) == _lib.GFD_EINVAL
+    assert lib.gfd_autotune_load(str(tmp_path / 'missing.txt').encode()) == _lib.GFD_EINVAL
+    assert lib.gfd_autotune_count(ctypes.byref(n)) == 0 and n.value == 2
+    assert lib.gfd_autotune_clear() == 0
+    assert lib.gfd_autotune_count(ctypes.byref(n)) == 0 and n.value == 0
