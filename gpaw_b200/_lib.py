@@ -95,6 +95,7 @@ SIGNATURES = {
     'gfd_poisson_batch_create': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp),
                                                 ctypes.POINTER(_vp)]),
     'gfd_poisson_batch_destroy': (ctypes.c_int, [_vp]),
+    'gfd_poisson_batch_grouped': (ctypes.c_int, [_vp, _ip]),
     'gfd_poisson_batch_solve_async': (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                                      ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                      _vp]),

@@ -33,35 +33,10 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "poisson_internal.h"
 #include "util.cuh"
 
 namespace {
-
-struct Level {
-  gfd_operator* op = nullptr;
-  int64_t n = 0;
-  void* phi[2] = {nullptr, nullptr};
-  void* rho = nullptr;
-  void* res = nullptr;
-  int pre = 0, post = 0;
-  double w = 1.0;
-};
-
-// Solve controls shared by host and device.  The host writes the inputs
-// before each launch and reads the outputs after it.
-struct SolveCtrl {
-  double eps;
-  double maxcharge;
-  double charge_arg;  // NaN: use the integral of rho
-  int maxiter;
-  int pad0;
-  double charge;      // integral of rho times dv
-  double bg;          // background charge density removed from rho
-  double err;         // last residual norm sum(r^2) dv
-  double sum;         // scratch scalar (sum of phi)
-  int niter;
-  int status;         // GFD_OK or GFD_EUNSUPPORTED (charged)
-};
 
 __global__ void prep_kernel(SolveCtrl* c, double npoints, double dv,
                             cudaGraphConditionalHandle loop, int in_graph) {
@@ -103,31 +78,6 @@ __global__ void __launch_bounds__(256) sub_mean_kernel(double* phi, const SolveC
 
 }  // namespace
 
-struct gfd_poisson {
-  int levels = 0;
-  std::vector<gfd_transformer*> restr, interp;
-  int relax_method = GFD_RELAX_JACOBI;
-  double dv = 1.0;
-  int pbc_all = 0;
-  int precision = GFD_POISSON_FP64;
-  std::vector<Level> L;     // hierarchy in the V-cycle precision
-  int vdtype = GFD_FLOAT64; // dtype of the V-cycle arrays
-  // Float64 fine-grid arrays: the caller's rho and phi are copied here.
-  double* rho_in = nullptr;
-  double* phi64 = nullptr;  // mixed form: the float64 potential
-  double* rho64 = nullptr;  // mixed form: rho - background
-  double* r64 = nullptr;    // mixed form: float64 residual
-  double* partials = nullptr;
-  int64_t npartials = 0;
-  SolveCtrl* dctrl = nullptr;
-  SolveCtrl* hctrl = nullptr;  // pinned
-  void* pool = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int device = -1;
-  gfd_operator* B = nullptr;  // Mehrstellen right-hand side (not owned)
-};
-
 namespace gfd {
 
 static int relax_level(gfd_poisson* ps, Level& lv, int& cur, int nsweeps, cudaStream_t s) {
@@ -155,6 +105,8 @@ static bool seedable(const gfd_poisson* ps, int l) {
          (l < ps->levels ? lv.pre > 0 : lv.post > 0);
 }
 static double seed_scale(const Level& lv) { return lv.w / lv.op->c0; }
+bool poisson_seedable(const gfd_poisson* ps, int l) { return seedable(ps, l); }
+double poisson_seed_scale(const Level& lv) { return seed_scale(lv); }
 
 // Enqueue one V-cycle from level l down; every level starts in phi[0] and
 // ends there.  final_norm: the level-0 residual norm into dctrl->err.
@@ -229,6 +181,31 @@ static int rhs_launch(gfd_poisson* ps, cudaStream_t s) {
   int st = check_launch("sub_bg_kernel");
   if (st || !ps->B) return st;
   return op_launch(ps->B, GFD_FLOAT64, OP_APPLY, dst, rho0, nullptr, 1, nullptr, 0.0, nullptr, s);
+}
+
+int poisson_prologue(gfd_poisson* ps, cudaStream_t s) {
+  const int64_t n0 = ps->L[0].n;
+  int st;
+  if ((st = reduce_launch(GFD_FLOAT64, ps->rho_in, n0, false, ps->dv, ps->partials,
+                          &ps->dctrl->charge, s)))
+    return st;
+  launch_k(prep_kernel, 1, 1, 0, s, ps->dctrl, double(n0), ps->dv,
+           cudaGraphConditionalHandle(0), 0);
+  if ((st = check_launch("prep_kernel"))) return st;
+  return rhs_launch(ps, s);
+}
+
+int poisson_epilogue(gfd_poisson* ps, cudaStream_t s) {
+  if (!ps->pbc_all) return GFD_OK;
+  const int64_t n0 = ps->L[0].n;
+  double* phi_final = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
+                                                        : ps->phi64;
+  int st;
+  if ((st = reduce_launch(GFD_FLOAT64, phi_final, n0, false, 1.0, ps->partials, &ps->dctrl->sum,
+                          s)))
+    return st;
+  launch_k(sub_mean_kernel, grid_for(n0), 256, 0, s, phi_final, ps->dctrl, (long long)n0);
+  return check_launch("sub_mean_kernel");
 }
 
 // Body of the solve loop: one iteration of the chosen form, ending with the
@@ -360,10 +337,18 @@ static void abort_capture(cudaStream_t cs) {
   cudaGetLastError();
 }
 
-// Capture the graphs of n solvers as independent branches of one graph (one
-// solver: that solver's own graph).
-static int build_multi_graph(gfd_poisson* const* solvers, int n, cudaGraph_t* graph_out,
-                             cudaGraphExec_t* exec_out) {
+// One branch of a batch graph: a solver alone, or a group of solvers whose
+// V-cycle steps run as single launches (poisson_group.cu).
+struct BatchUnit {
+  gfd_poisson* ps = nullptr;
+  gfd::PoissonGroup* group = nullptr;
+};
+
+// Capture the units as independent branches of one graph (one solver: that
+// solver's own graph).
+static int build_unit_graph(const std::vector<BatchUnit>& units, cudaGraph_t* graph_out,
+                            cudaGraphExec_t* exec_out) {
+  const int n = (int)units.size();
   std::vector<cudaStream_t> cs(n + 1, nullptr);
   for (auto& c : cs) {
     int st = check_cuda(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -387,7 +372,9 @@ static int build_multi_graph(gfd_poisson* const* solvers, int n, cudaGraph_t* gr
   if (!st) st = check_cuda(cudaEventRecord(fork, origin), "cudaEventRecord");
   for (int i = 0; i < n && !st; i++) {
     st = check_cuda(cudaStreamWaitEvent(cs[i], fork, 0), "cudaStreamWaitEvent");
-    if (!st) st = capture_solve(solvers[i], cs[i], &bodies[i], &loops[i]);
+    if (!st)
+      st = units[i].group ? group_capture_outer(units[i].group, cs[i], &bodies[i], &loops[i])
+                          : capture_solve(units[i].ps, cs[i], &bodies[i], &loops[i]);
     if (!st) st = check_cuda(cudaEventRecord(join[i], cs[i]), "cudaEventRecord");
     if (!st) st = check_cuda(cudaStreamWaitEvent(origin, join[i], 0), "cudaStreamWaitEvent");
   }
@@ -396,7 +383,9 @@ static int build_multi_graph(gfd_poisson* const* solvers, int n, cudaGraph_t* gr
   } else {
     st = check_cuda(cudaStreamEndCapture(origin, &graph), "cudaStreamEndCapture");
   }
-  for (int i = 0; i < n && !st; i++) st = capture_body(solvers[i], cs[0], bodies[i], loops[i]);
+  for (int i = 0; i < n && !st; i++)
+    st = units[i].group ? group_capture_body(units[i].group, cs[0], bodies[i], loops[i])
+                        : capture_body(units[i].ps, cs[0], bodies[i], loops[i]);
   if (!st) {
     cudaGraphExec_t exec = nullptr;
     st = check_cuda(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
@@ -410,6 +399,13 @@ static int build_multi_graph(gfd_poisson* const* solvers, int n, cudaGraph_t* gr
   for (auto& e : join) if (e) cudaEventDestroy(e);
   for (auto& c : cs) cudaStreamDestroy(c);
   return st;
+}
+
+static int build_multi_graph(gfd_poisson* const* solvers, int n, cudaGraph_t* graph_out,
+                             cudaGraphExec_t* exec_out) {
+  std::vector<BatchUnit> units(n);
+  for (int i = 0; i < n; i++) units[i].ps = solvers[i];
+  return build_unit_graph(units, graph_out, exec_out);
 }
 
 static int build_graph(gfd_poisson* ps) {
@@ -730,7 +726,18 @@ struct gfd_poisson_batch {
   std::vector<gfd_poisson*> solvers;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  std::vector<gfd::PoissonGroup*> groups;  // solvers of one structure, grouped
+  int grouped = 0;                         // solvers inside groups
 };
+
+// GFD_BATCH_GROUPED=0: batches always use one graph branch per solver.
+static bool grouping_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("GFD_BATCH_GROUPED");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 
 extern "C" int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solvers,
                                         gfd_poisson_batch** out) {
@@ -746,8 +753,35 @@ extern "C" int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solver
   gfd_poisson_batch* b = new (std::nothrow) gfd_poisson_batch();
   if (!b) return set_error(GFD_ENOMEM, "host allocation failed");
   b->solvers.assign(solvers, solvers + nsolvers);
-  int st = build_multi_graph(b->solvers.data(), nsolvers, &b->graph, &b->exec);
+  // Solvers of one structure form a group; the rest run alone.
+  std::vector<std::vector<gfd_poisson*>> parts;
+  for (gfd_poisson* s : b->solvers) {
+    bool placed = false;
+    if (grouping_enabled() && gfd::group_eligible(s) && gfd::group_same_structure(s, s, nullptr))
+      for (auto& part : parts)
+        if (gfd::group_same_structure(part[0], s, nullptr)) {
+          part.push_back(s);
+          placed = true;
+          break;
+        }
+    if (!placed) parts.push_back({s});
+  }
+  std::vector<BatchUnit> units;
+  int st = GFD_OK;
+  for (auto& part : parts) {
+    BatchUnit u;
+    if (part.size() >= 2) {
+      if ((st = gfd::group_create(part.data(), (int)part.size(), &u.group))) break;
+      b->groups.push_back(u.group);
+      b->grouped += (int)part.size();
+    } else {
+      u.ps = part[0];
+    }
+    units.push_back(u);
+  }
+  if (!st) st = build_unit_graph(units, &b->graph, &b->exec);
   if (st) {
+    for (auto* g : b->groups) gfd::group_destroy(g);
     delete b;
     return st;
   }
@@ -759,6 +793,7 @@ extern "C" int gfd_poisson_batch_destroy(gfd_poisson_batch* b) {
   if (!b) return GFD_OK;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto* g : b->groups) gfd::group_destroy(g);
   delete b;
   return GFD_OK;
 }
@@ -780,5 +815,11 @@ extern "C" int gfd_poisson_batch_solve_async(gfd_poisson_batch* b, double* const
   if ((st = check_cuda(cudaGraphLaunch(b->exec, s), "cudaGraphLaunch(batch)"))) return st;
   for (int i = 0; i < n; i++)
     if ((st = stage_out(b->solvers[i], phis[i], s))) return st;
+  return GFD_OK;
+}
+
+extern "C" int gfd_poisson_batch_grouped(const gfd_poisson_batch* b, int* grouped) {
+  if (!b || !grouped) return set_error(GFD_EINVAL, "null argument");
+  *grouped = b->grouped;
   return GFD_OK;
 }

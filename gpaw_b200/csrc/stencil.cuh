@@ -589,33 +589,59 @@ general_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restric
 // axes are read from `frozen`, a copy taken at the start of the sweep, as
 // the reference's halo is filled once per sweep (c/operators.c:66-78).
 // ---------------------------------------------------------------------------
+// The update of point (i0, i1, i2).  phi and frozen may be the same array
+// (no periodic axis).
+template <class V>
+__device__ __forceinline__ void gs_point_at(V* phi, const V* __restrict__ rho, const V* frozen,
+                                            const GenParams<typename vt<V>::S>& p, int i0, int i1,
+                                            int i2) {
+  using S = typename vt<V>::S;
+  S s = 0;
+  for (int c = 1; c < p.ncoefs; c++) {
+    int sd0, sd1, sd2;
+    int j0 = wrap_axis(i0 + p.off[c][0], p.n0, p.per0, sd0);
+    int j1 = wrap_axis(i1 + p.off[c][1], p.n1, p.per1, sd1);
+    int j2 = wrap_axis(i2 + p.off[c][2], p.n2, p.per2, sd2);
+    if (j0 < 0 || j1 < 0 || j2 < 0) continue;
+    long long gg = ((long long)j0 * p.n1 + j1) * p.n2 + j2;
+    bool wrapped = (sd0 >= 0) || (sd1 >= 0) || (sd2 >= 0);
+    S v = wrapped ? frozen[gg] : phi[gg];
+    s += v * p.coefs[c];
+  }
+  const long long g = ((long long)i0 * p.n1 + i1) * p.n2 + i2;
+  phi[g] = (rho[g] - s) * (S(1) / p.coefs[0]);
+}
+
+// Points of one colour, enumerated without idle threads: index q covers
+// the rows (i0, i1) times gs_row_slots() slots; slot j of a row is
+// i2 = first + ncolor j, first = (color - i0 - i1) mod ncolor.  False for
+// slots past the row's end.  32-bit index arithmetic (a grid holds fewer
+// than 2^31 points).
+__host__ __device__ inline int gs_row_slots(int n2, int ncolor) {
+  return (n2 + ncolor - 1) / ncolor;
+}
+__device__ __forceinline__ bool gs_colour_point(int q, int slots, int ncolor, int color, int n1,
+                                                int n2, int& i0, int& i1, int& i2) {
+  const int row = q / slots, j = q - row * slots;
+  i0 = row / n1;
+  i1 = row - i0 * n1;
+  int first = (color - i0 - i1) % ncolor;
+  if (first < 0) first += ncolor;
+  i2 = first + ncolor * j;
+  return i2 < n2;
+}
+
 template <class V>
 __global__ void __launch_bounds__(256)
-color_gs_kernel(V* __restrict__ phi, const V* __restrict__ rho, const V* __restrict__ frozen,
+color_gs_kernel(V* phi, const V* __restrict__ rho, const V* frozen,
                 const GenParams<typename vt<V>::S> p, int ncolor, int color) {
   pdl_enter();
-  using S = typename vt<V>::S;
-  const long long n = (long long)p.n0 * p.n1 * p.n2;
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n;
-       g += (long long)gridDim.x * blockDim.x) {
-    int i2 = int(g % p.n2);
-    long long r = g / p.n2;
-    int i1 = int(r % p.n1);
-    int i0 = int(r / p.n1);
-    if ((i0 + i1 + i2) % ncolor != color) continue;
-    S s = 0;
-    for (int c = 1; c < p.ncoefs; c++) {
-      int sd0, sd1, sd2;
-      int j0 = wrap_axis(i0 + p.off[c][0], p.n0, p.per0, sd0);
-      int j1 = wrap_axis(i1 + p.off[c][1], p.n1, p.per1, sd1);
-      int j2 = wrap_axis(i2 + p.off[c][2], p.n2, p.per2, sd2);
-      if (j0 < 0 || j1 < 0 || j2 < 0) continue;
-      long long gg = ((long long)j0 * p.n1 + j1) * p.n2 + j2;
-      bool wrapped = (sd0 >= 0) || (sd1 >= 0) || (sd2 >= 0);
-      S v = wrapped ? frozen[gg] : phi[gg];
-      s += v * p.coefs[c];
-    }
-    phi[g] = (rho[g] - s) * (S(1) / p.coefs[0]);
+  const int slots = gs_row_slots(p.n2, ncolor);
+  const int nq = p.n0 * p.n1 * slots;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    int i0, i1, i2;
+    if (gs_colour_point(q, slots, ncolor, color, p.n1, p.n2, i0, i1, i2))
+      gs_point_at<V>(phi, rho, frozen, p, i0, i1, i2);
   }
 }
 

@@ -394,11 +394,10 @@ inline int64_t partials_count(const gfd_operator* op, int64_t nin) {
   return (int64_t)gx * gy * g.nxc * nin;
 }
 
-template <class V>
-int gs_typed(const gfd_operator* op, V* phi, const V* rho, int nsweeps, V* frozen, int ncolor,
-             cudaStream_t s) {
-  using S = typename vt<V>::S;
-  GenParams<S> p{};
+// Stencil parameters of a Gauss-Seidel colour pass (any offset set).
+template <class S>
+void gs_params(const gfd_operator* op, GenParams<S>& p) {
+  p = GenParams<S>{};
   p.n0 = op->n[0]; p.n1 = op->n[1]; p.n2 = op->n[2];
   p.per0 = op->per[0]; p.per1 = op->per[1]; p.per2 = op->per[2];
   p.band = (long long)op->n[0] * op->n[1] * op->n[2];
@@ -407,9 +406,18 @@ int gs_typed(const gfd_operator* op, V* phi, const V* rho, int nsweeps, V* froze
     p.coefs[c] = S(op->coefs[c]);
     for (int a = 0; a < 3; a++) p.off[c][a] = (signed char)op->off[3 * c + a];
   }
+}
+
+template <class V>
+int gs_typed(const gfd_operator* op, V* phi, const V* rho, int nsweeps, V* frozen, int ncolor,
+             cudaStream_t s) {
+  using S = typename vt<V>::S;
+  GenParams<S> p;
+  gs_params(op, p);
   const long long n = p.band;
   const bool any_per = op->per[0] || op->per[1] || op->per[2];
-  int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  const long long nq = (long long)op->n[0] * op->n[1] * gs_row_slots(op->n[2], ncolor);
+  int blocks = (int)std::min<long long>((nq + 255) / 256, 148LL * 16);
   for (int sw = 0; sw < nsweeps; sw++) {
     if (any_per) {
       cudaError_t e = cudaMemcpyAsync(frozen, phi, n * sizeof(V), cudaMemcpyDeviceToDevice, s);

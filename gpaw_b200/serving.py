@@ -31,7 +31,13 @@ from .poisson import PoissonSolver
 
 
 class PoissonBatch:
-    """Independent solves launched together (one graph, parallel branches)."""
+    """Independent solves launched together as one graph.  Solvers of one
+    structure (same levels, smoothing, stencil and transfer orders and
+    boundary conditions; any grid sizes; float64) run grouped: each V-cycle
+    step is one persistent launch over all their grids, pulling work tiles
+    from a queue, and each solve stops on its own criterion.  Groups and the
+    other solvers run as parallel graph branches.  `grouped`: how many
+    solvers run inside groups."""
 
     def __init__(self, solvers):
         self.solvers = list(solvers)
@@ -43,6 +49,9 @@ class PoissonBatch:
         _lib.check(_lib.lib.gfd_poisson_batch_create(len(self.solvers), handles,
                                                      _lib.ctypes.byref(h)), 'PoissonBatch')
         self.batch = h
+        g = _lib.ctypes.c_int(0)
+        _lib.check(_lib.lib.gfd_poisson_batch_grouped(h, _lib.ctypes.byref(g)))
+        self.grouped = g.value
 
     def __del__(self):
         h = getattr(self, 'batch', None)

@@ -274,6 +274,15 @@ GFD_API int gfd_poisson_batch_destroy(gfd_poisson_batch* batch);
 GFD_API int gfd_poisson_batch_solve_async(gfd_poisson_batch* batch, double* const* phis,
                                           const double* const* rhos, double eps, double maxcharge,
                                           int maxiter, void* stream);
+/* *grouped = how many of the batch's solvers run grouped.  Solvers of one
+ * structure (levels, smoothing, weights, stencil radius or colouring and
+ * boundary conditions per level, transfer orders; float64, no Mehrstellen
+ * right-hand side) form a group: every V-cycle step is ONE launch over all
+ * the group's grids, a persistent kernel whose CTAs pull work tiles from a
+ * queue, and the stopping rule runs per solve on the device.  Groups and the
+ * remaining solvers run as parallel graph branches (all solvers alone with
+ * GFD_BATCH_GROUPED=0). */
+GFD_API int gfd_poisson_batch_grouped(const gfd_poisson_batch* batch, int* grouped);
 
 /* ------------------------------------------------------------------------
  * Launch-plan autotuning.  No counterpart in the reference, whose CPU code

@@ -57,6 +57,132 @@ def test_batch_of_uneven_grids(cuda):
     assert all(torch.equal(a, b) for a, b in zip(phis, phis2))
 
 
+def make_batch(cuda, sizes, relax='J', precision='fp64', seed=300):
+    import torch
+    from gpaw_b200.poisson import PoissonSolver
+    from gpaw_b200.serving import PoissonBatch, grid_for, pair_density
+    solvers, rhos = [], []
+    for i, N in enumerate(sizes):
+        ps = PoissonSolver(3, relax, 2e-10, precision=precision)
+        ps.set_grid_descriptor(grid_for(N, H, device=cuda))
+        ps.initialize()
+        solvers.append(ps)
+        rhos.append(pair_density(grid_for(N, H, device=cuda), seed + i))
+    return PoissonBatch(solvers), solvers, rhos
+
+
+def solve_alone(cuda, N, rho, relax='J', precision='fp64', eps=2e-10):
+    import torch
+    from gpaw_b200.poisson import PoissonSolver
+    from gpaw_b200.serving import grid_for
+    ps = PoissonSolver(3, relax, eps, precision=precision)
+    ps.set_grid_descriptor(grid_for(N, H, device=cuda))
+    phi = torch.zeros_like(rho)
+    n = ps.solve(phi, rho)
+    return phi, n
+
+
+@pytest.mark.parametrize('relax', ['J', 'GS'])
+def test_grouped_batch_matches_alone(cuda, relax):
+    """Small solvers of one structure are grouped: one launch per V-cycle
+    step over all their grids.  Here 24^3 (three coarsenings) and 32^3 (four)
+    form two groups; 20^3 (two coarsenings) and 48^3 (above the 32768-point
+    default) run alone beside them.  Every result equals the solve alone bit
+    for bit, and the oracle's (Jacobi: same V-cycle count, 1e-10)."""
+    import torch
+    sizes = [24, 32, 20, 24, 48, 32]
+    batch, solvers, rhos = make_batch(cuda, sizes, relax)
+    assert batch.grouped == 4
+    phis = [torch.zeros_like(r) for r in rhos]
+    res = batch.solve(phis, rhos)
+    for i, N in enumerate(sizes):
+        phi, n = solve_alone(cuda, N, rhos[i], relax)
+        assert n == res[i][0], (N, n, res[i][0])
+        assert res[i][1] <= 2e-10
+        assert torch.equal(phi, phis[i]), N
+        if relax == 'J' and N <= 48:
+            phi_o, n_o = oracle_solve(N, rhos[i].cpu().numpy())
+            assert n == n_o
+            assert np.abs(phis[i].cpu().numpy() - phi_o).max() < 1e-10
+    phis2 = [torch.zeros_like(r) for r in rhos]
+    res2 = batch.solve(phis2, rhos)
+    assert [r[0] for r in res2] == [r[0] for r in res]
+    assert all(torch.equal(a, b) for a, b in zip(phis, phis2))
+
+
+_LARGE_GROUP = r"""
+import sys, torch
+sys.path.insert(0, 'tests')
+from test_gpu_serving import make_batch, solve_alone
+for relax in ('J', 'GS'):
+    sizes = [48, 80, 64]
+    batch, solvers, rhos = make_batch('cuda', sizes, relax, seed=700)
+    assert batch.grouped == 3, batch.grouped
+    phis = [torch.zeros_like(r) for r in rhos]
+    res = batch.solve(phis, rhos)
+    for i, N in enumerate(sizes):
+        phi, n = solve_alone('cuda', N, rhos[i], relax)
+        assert n == res[i][0], (relax, N, n, res[i][0])
+        d = float((phi - phis[i]).abs().max()) / float(phi.abs().max())
+        assert d < 1e-12, (relax, N, d)
+print('ok')
+"""
+
+
+def test_grouped_batch_with_large_grids(cuda):
+    """GFD_GROUP_MAX_POINTS raises the size limit: 48^3 to 80^3 join the
+    group; 80^3 runs one-thread-per-point kernels where alone it marches, so
+    it matches the solve alone to rounding (1e-12 relative), same count."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, GFD_GROUP_MAX_POINTS='100000000')
+    r = subprocess.run([sys.executable, '-c', _LARGE_GROUP], cwd=root, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and 'ok' in r.stdout, r.stdout + r.stderr
+
+
+def test_grouped_batch_charged_and_maxiter(cuda):
+    """Per-solve outcomes inside one grouped launch: a charged request is
+    refused (NotImplementedError) without touching the others, and maxiter
+    stops every solve at that count (PoissonConvergenceError)."""
+    import torch
+    from gpaw_b200.errors import PoissonConvergenceError
+    sizes = [32, 32, 32]
+    batch, solvers, rhos = make_batch(cuda, sizes, seed=410)
+    assert batch.grouped == 3
+    rhos[1] = rhos[1] + 1e-3          # net charge
+    phis = [torch.zeros_like(r) for r in rhos]
+    with pytest.raises(NotImplementedError):
+        batch.solve(phis, rhos)
+    for i in (0, 2):
+        n, err = solvers[i].result()
+        phi, n_alone = solve_alone(cuda, sizes[i], rhos[i])
+        assert n == n_alone and err <= 2e-10
+        assert torch.equal(phi, phis[i])
+    rhos[1] = rhos[1] - rhos[1].mean()
+    phis = [torch.zeros_like(r) for r in rhos]
+    with pytest.raises(PoissonConvergenceError):
+        batch.solve(phis, rhos, maxiter=2)
+    for s in solvers:
+        with pytest.raises(PoissonConvergenceError):
+            s.result()
+        assert s.niter == 2
+
+
+def test_mixed_precision_batch_uses_branches(cuda):
+    import torch
+    sizes = [24, 32]
+    batch, solvers, rhos = make_batch(cuda, sizes, precision='mixed', seed=500)
+    assert batch.grouped == 0
+    phis = [torch.zeros_like(r) for r in rhos]
+    res = batch.solve(phis, rhos)
+    for i, N in enumerate(sizes):
+        phi, n = solve_alone(cuda, N, rhos[i], precision='mixed')
+        assert n == res[i][0] and torch.equal(phi, phis[i])
+
+
 @pytest.mark.parametrize('precision', ['fp64', 'mixed'])
 def test_server_alone_vs_mix(cuda, precision):
     import torch
