@@ -305,7 +305,10 @@ SERVING_SIZES = (32, 48, 64, 96, 128, 160)
 
 
 def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=300,
-                  precisions=('fp64', 'mixed'), seed=5):
+                  precisions=('fp64', 'mixed'), seed=5, seconds=2.5, max_req=3000):
+    """Requests per rate: about `seconds` of arrivals, at least nreq and at
+    most max_req (the full 10,000-request stream would take minutes at the
+    low rates)."""
     import torch
     from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
     h = 0.2 / BOHR
@@ -315,21 +318,24 @@ def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=300,
     dens = {N: [pair_density(grid_for(N, h), 1000 * N + k) for k in range(4)]
             for N in SERVING_SIZES}
     torch.cuda.synchronize()
-    out = {'workload': '%d requests per rate, grids %s^3 zero boundary, h=0.2 A, pair densities, '
-                       'eps=2e-10, budget 120 GB' % (nreq, list(SERVING_SIZES))}
+    out = {'workload': 'max(%d, min(%d, %.1f s x rate)) requests per rate, grids %s^3 zero '
+                       'boundary, h=0.2 A, pair densities, eps=2e-10, budget 120 GB'
+                       % (nreq, max_req, seconds, list(SERVING_SIZES))}
     for prec in precisions:
         srv = PoissonServer(h, precision=prec, max_inflight=64, nstreams=32)
         srv.warm(SERVING_SIZES, per_size=24)
         res = {}
         for lam in rates:
-            gaps = rng.exponential(1.0 / lam, nreq)
+            m = int(min(max_req, max(nreq, lam * seconds)))
+            gaps = rng.exponential(1.0 / lam, m)
             t = np.cumsum(gaps) - gaps[0]
-            sizes = rng.choice(SERVING_SIZES, nreq)
+            sizes = rng.choice(SERVING_SIZES, m)
             reqs = [Request(i, int(N), float(t[i]), dens[int(N)][i % 4]) for i, N in enumerate(sizes)]
             srv.run(reqs[:16])  # warm the pools for this rate (not timed)
             stats = srv.run(reqs)
-            res['%g/s' % lam] = {k: stats[k] for k in ('completed', 'solves_per_s', 'p50_ms',
-                                                         'p99_ms', 'max_err', 'rejected')}
+            res['%g/s' % lam] = {k: stats[k] for k in ('requests', 'completed', 'solves_per_s',
+                                                         'p50_ms', 'p99_ms', 'max_err',
+                                                         'rejected')}
         res['device_bytes'] = srv.used_bytes
         out[prec] = res
     return out
