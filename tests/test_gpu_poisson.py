@@ -122,6 +122,39 @@ def test_convergence_error_and_charged(cuda):
         ps.solve(phi, dev(rho + 1.0, cuda))
 
 
+@pytest.mark.parametrize('relax,tol', [('J', 6e-16), ('GS', 3e-6)])
+def test_poisson_symmetry(cuda, relax, tol):
+    """gpaw/test/poisson.py:8-41: on a periodic 16^3 grid (cell 2.87 A) two
+    identical charge blobs at (0, 0, 0) and the cell centre give a potential
+    with phi[0, 0, 0] == phi[8, 8, 8] (nn = 1, charge = 0 passed).  The
+    reference builds its blobs with an l = 0 spline through localized
+    functions; here the same profile is laid on the grid directly: the line
+    through the spline's points (0, 1), (rc/2, 0.5), (rc, 0) times Y_00,
+    rc = 0.9 N / 2 grid spacings.  Tolerances as the reference's."""
+    import torch
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.poisson import PoissonSolver
+    N, L = 16, 2.87 / 0.529177
+    gd = GridDescriptor((N,) * 3, (L,) * 3)
+    h = L / N
+    rc = N / 2.0 * 0.9 * h
+    i = np.arange(N)
+    a = np.zeros((N,) * 3)
+    for centre in (0, N // 2):
+        d = np.minimum(np.abs(i - centre), N - np.abs(i - centre)) * h  # minimum image
+        r2 = d[:, None, None] ** 2 + d[None, :, None] ** 2 + d[None, None, :] ** 2
+        # the spline through (0, 1), (rc/2, 0.5), (rc, 0) times Y_00
+        a += np.where(r2 < rc * rc, 1 - np.sqrt(r2) / rc, 0.0) / np.sqrt(4 * np.pi)
+    a -= a.mean()
+    ps = PoissonSolver(1, relax, 2e-10)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    b = torch.zeros((N,) * 3, dtype=torch.float64, device=cuda)
+    ps.solve(b, dev(a, cuda), charge=0)
+    b = b.cpu().numpy()
+    assert abs(b[0, 0, 0] - b[8, 8, 8]) < tol
+
+
 def test_gauss_multipoles(cuda):
     """gpaw/test/gauss_func.py:13-78: nn=3, N=48 zero boundary, cell 20 Bohr;
     the potential of Gaussian multipoles L = 0..6 against the analytic one,
