@@ -133,6 +133,36 @@ constexpr int rst_pitch() {
   return rst_half<V, RZ>() + RZ / 2;
 }
 
+// Types up to 8 bytes: each thread restricts two neighbouring coarse
+// columns at once, and a staged fine row is kept in four phases (position
+// mod 4), phase q at q * QS + position / 4.  The 2nn + 1 taps of the pair
+// (even positions) and its two centres (odd ones) are then consecutive
+// words across lanes: 2nn + 3 loads per pair instead of 2 (2nn + 1).  QS is
+// E / 4 past a 128-byte segment start (E / 4 elements mod E), so the four
+// phase runs one wavefront writes use each bank at most twice.
+template <class V, int RZ>
+constexpr int rst_quad() {
+  constexpr int E = 128 / int(sizeof(V));
+  int q = (RZ + 3) / 4;
+  while (q % E != E / 4) ++q;
+  return q;
+}
+template <class V>
+constexpr bool rst_pairs() {
+  return sizeof(V) <= 8;
+}
+// Shared-memory row pitch of a staged fine row (elements).
+template <class V, int RZ>
+constexpr int rst_row_pitch() {
+  if constexpr (rst_pairs<V>()) return 4 * rst_quad<V, RZ>();
+  else return rst_pitch<V, RZ>();
+}
+
+template <class V>
+struct alignas(2 * sizeof(V)) VPair {
+  V a, b;
+};
+
 // ---------------------------------------------------------------------------
 // Restriction: coarse index i on an axis takes the fine padded point
 // (K-1) + 2i (c/bmgs/restrict.c:65-69), i.e. fine array index
@@ -154,9 +184,12 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
   // Each staged fine row holds its even positions first, then its odd ones:
   // the axis-2 taps of neighbouring coarse points are then consecutive
   // words (a stride-2 read would hit every bank twice).
-  constexpr int HALF = rst_half<V, RZ>(), RZP = rst_pitch<V, RZ>(), STG = RY * RZP;
+  constexpr bool PAIRS = rst_pairs<V>();
+  constexpr int HALF = rst_half<V, RZ>(), QS = rst_quad<V, RZ>();
+  constexpr int RZP = rst_row_pitch<V, RZ>(), STG = RY * RZP;
+  static_assert(!PAIRS || BZC % 2 == 0, "coarse columns come in pairs");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZP], rows de-interleaved
+  V* F = reinterpret_cast<V*>(smem_raw);          // [2][RY][RZP], rows in phases
   V* T = F + 2 * STG;                             // [2][RY][BZC]
 
   const int t = threadIdx.x, tz = t % BZC, ty = t / BZC;
@@ -178,7 +211,8 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
     dpos[i] = 0;
     if (c < CELLS) {
       int sy = c / RZ, sz = c % RZ;
-      dpos[i] = sy * RZP + ((sz & 1) ? HALF + (sz >> 1) : (sz >> 1));
+      if constexpr (PAIRS) dpos[i] = sy * RZP + (sz & 3) * QS + (sz >> 2);
+      else dpos[i] = sy * RZP + ((sz & 1) ? HALF + (sz >> 1) : (sz >> 1));
       int ysd, zsd;
       int ys = wrap_axis(fy0 + sy, p.ni1, p.per1, ysd);
       int zs = wrap_axis(fz0 + sz, p.ni2, p.per2, zsd);
@@ -219,12 +253,31 @@ restrict_kernel(const V* __restrict__ in, V* __restrict__ out,
       if (t + i * NT < CELLS) Fb[dpos[i]] = rv[i];
     load(f + 1);
     __syncthreads();
-    // axis-2 pass: Tb[sy][cz] for every staged row; fine position
-    // 2 cz + W + o sits at (W + o) & 1 ? HALF : 0, + cz + (W + o) / 2.
-    for (int c = t; c < RY * BZC; c += NT) {
-      const int sy = c / BZC, cz = c % BZC;
-      const V* row = Fb + sy * RZP + cz;
-      Tb[c] = rst_tap<NN, V>([&](int o) { return row[((W + o) & 1 ? HALF : 0) + ((W + o) >> 1)]; });
+    if constexpr (PAIRS) {
+      // axis-2 pass, columns cz = 2m and 2m + 1 of every staged row: their
+      // taps are fine positions 4m + 2j (j = 0 .. 2nn; j = 0 .. 2nn - 1 for
+      // cz = 2m, 1 .. 2nn for 2m + 1), their centres 4m + W and 4m + W + 2.
+      for (int c = t; c < RY * (BZC / 2); c += NT) {
+        const int sy = c / (BZC / 2), m = c % (BZC / 2);
+        const V* row = Fb + sy * RZP + m;
+        V tap[2 * NN + 1];
+#pragma unroll
+        for (int j = 0; j <= 2 * NN; j++) tap[j] = row[((2 * j) & 3) * QS + (j >> 1)];
+        const V c0 = row[(W & 3) * QS + (W >> 2)];
+        const V c1 = row[((W + 2) & 3) * QS + ((W + 2) >> 2)];
+        VPair<V> r;
+        r.a = rst_tap<NN, V>([&](int o) { return o == 0 ? c0 : tap[(o + W) >> 1]; });
+        r.b = rst_tap<NN, V>([&](int o) { return o == 0 ? c1 : tap[((o + W) >> 1) + 1]; });
+        *reinterpret_cast<VPair<V>*>(Tb + sy * BZC + 2 * m) = r;
+      }
+    } else {
+      // axis-2 pass: Tb[sy][cz] for every staged row; fine position
+      // 2 cz + W + o sits at (W + o) & 1 ? HALF : 0, + cz + (W + o) / 2.
+      for (int c = t; c < RY * BZC; c += NT) {
+        const int sy = c / BZC, cz = c % BZC;
+        const V* row = Fb + sy * RZP + cz;
+        Tb[c] = rst_tap<NN, V>([&](int o) { return row[((W + o) & 1 ? HALF : 0) + ((W + o) >> 1)]; });
+      }
     }
     __syncthreads();
     // axis-1 pass for this thread's coarse points, pushed into the queue

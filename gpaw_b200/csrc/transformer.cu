@@ -18,7 +18,7 @@ static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t n
   constexpr int BZC = 32, TYC = 8, VYC = sizeof(V) >= 16 ? 1 : 2, BYC = TYC * VYC;
   constexpr int W = 2 * NN - 1;
   constexpr int RY = 2 * BYC - 1 + 2 * W, RZ = 2 * BZC - 1 + 2 * W;
-  const size_t smem = (size_t)(2 * RY * rst_pitch<V, RZ>() + 2 * RY * BZC) * sizeof(V);
+  const size_t smem = (size_t)(2 * RY * rst_row_pitch<V, RZ>() + 2 * RY * BZC) * sizeof(V);
   const int gx = (tr->nout[2] + BZC - 1) / BZC, gy = (tr->nout[1] + BYC - 1) / BYC;
   const int64_t tiles = (int64_t)gx * gy * nin;
   const int64_t target = (int64_t)(cps > 0 ? cps : march_ctas_per_sm()) * num_sms();
