@@ -323,7 +323,7 @@ def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=300,
                        % (nreq, max_req, seconds, list(SERVING_SIZES))}
     for prec in precisions:
         srv = PoissonServer(h, precision=prec, max_inflight=64, nstreams=32)
-        srv.warm(SERVING_SIZES, per_size=24)
+        srv.warm(SERVING_SIZES, per_size=24, pod_requests=64)
         res = {}
         for lam in rates:
             m = int(min(max_req, max(nreq, lam * seconds)))

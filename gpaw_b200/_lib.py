@@ -33,6 +33,8 @@ GFD_RELAX_JACOBI = 2
 GFD_POISSON_FP64 = 0
 GFD_POISSON_MIXED = 1
 
+GFD_BATCH_NO_GROUPS = 1
+
 GFD_TUNE_APPLY = 0
 GFD_TUNE_JACOBI = 1
 GFD_TUNE_POTENTIAL = 3
@@ -95,6 +97,8 @@ SIGNATURES = {
     'gfd_poisson_batch_create': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp),
                                                 ctypes.POINTER(_vp)]),
     'gfd_poisson_batch_destroy': (ctypes.c_int, [_vp]),
+    'gfd_poisson_batch_create_ex': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int,
+                                                   ctypes.POINTER(_vp)]),
     'gfd_poisson_batch_grouped': (ctypes.c_int, [_vp, _ip]),
     'gfd_poisson_batch_solve_async': (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                                      ctypes.c_double, ctypes.c_double, ctypes.c_int,

@@ -741,6 +741,11 @@ static bool grouping_enabled() {
 
 extern "C" int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solvers,
                                         gfd_poisson_batch** out) {
+  return gfd_poisson_batch_create_ex(nsolvers, solvers, 0, out);
+}
+
+extern "C" int gfd_poisson_batch_create_ex(int nsolvers, gfd_poisson* const* solvers, int flags,
+                                           gfd_poisson_batch** out) {
   if (!out) return set_error(GFD_EINVAL, "null output handle");
   *out = nullptr;
   if (nsolvers < 1 || !solvers) return set_error(GFD_EINVAL, "a batch needs at least one solver");
@@ -757,7 +762,8 @@ extern "C" int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solver
   std::vector<std::vector<gfd_poisson*>> parts;
   for (gfd_poisson* s : b->solvers) {
     bool placed = false;
-    if (grouping_enabled() && gfd::group_eligible(s) && gfd::group_same_structure(s, s, nullptr))
+    if (!(flags & GFD_BATCH_NO_GROUPS) && grouping_enabled() && gfd::group_eligible(s) &&
+        gfd::group_same_structure(s, s, nullptr))
       for (auto& part : parts)
         if (gfd::group_same_structure(part[0], s, nullptr)) {
           part.push_back(s);
@@ -807,14 +813,31 @@ extern "C" int gfd_poisson_batch_solve_async(gfd_poisson_batch* b, double* const
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int n = (int)b->solvers.size();
   int st;
+  for (int i = 0; i < n; i++)
+    if (!phis[i] != !rhos[i])
+      return set_error(GFD_EINVAL, "phi and rho of a batch slot must both be given or both null");
   for (int i = 0; i < n; i++) {
-    if (!phis[i] || !rhos[i]) return set_error(GFD_EINVAL, "null array pointer in batch");
+    if (!phis[i]) {
+      // Unused slot: an infinite charge marks the solve as refused, so it
+      // runs no V-cycle; its arrays are neither read nor written.
+      gfd_poisson* ps = b->solvers[i];
+      SolveCtrl* h = ps->hctrl;
+      h->eps = eps;
+      h->maxcharge = maxcharge;
+      h->charge_arg = INFINITY;
+      h->maxiter = maxiter;
+      if ((st = check_cuda(cudaMemcpyAsync(ps->dctrl, h, offsetof(SolveCtrl, charge),
+                                           cudaMemcpyHostToDevice, s),
+                           "cudaMemcpyAsync(controls)")))
+        return st;
+      continue;
+    }
     if ((st = stage_in(b->solvers[i], phis[i], rhos[i], std::nan(""), eps, maxcharge, maxiter, s)))
       return st;
   }
   if ((st = check_cuda(cudaGraphLaunch(b->exec, s), "cudaGraphLaunch(batch)"))) return st;
   for (int i = 0; i < n; i++)
-    if ((st = stage_out(b->solvers[i], phis[i], s))) return st;
+    if (phis[i] && (st = stage_out(b->solvers[i], phis[i], s))) return st;
   return GFD_OK;
 }
 

@@ -87,8 +87,9 @@ class FDOperator:
 
     def __del__(self):
         h = getattr(self, 'operator', None)
-        if h:
-            _lib.lib.gfd_operator_destroy(h)
+        lib = getattr(_lib, 'lib', None) if _lib is not None else None
+        if h and lib is not None:  # at interpreter exit the module may be gone
+            lib.gfd_operator_destroy(h)
             self.operator = None
 
     def _check_arrays(self, a, b):

@@ -115,8 +115,9 @@ class PoissonSolver:
 
     def __del__(self):
         h = getattr(self, 'solver', None)
-        if h:
-            _lib.lib.gfd_poisson_destroy(h)
+        lib = getattr(_lib, 'lib', None) if _lib is not None else None
+        if h and lib is not None:  # at interpreter exit the module may be gone
+            lib.gfd_poisson_destroy(h)
             self.solver = None
 
     def solve(self, phi, rho, charge=None, eps=None, maxcharge=1e-6, zero_initial_phi=False):

@@ -60,8 +60,9 @@ class Preconditioner:
 
     def __del__(self):
         h = getattr(self, 'handle', None)
-        if h:
-            _lib.lib.gfd_preconditioner_destroy(h)
+        lib = getattr(_lib, 'lib', None) if _lib is not None else None
+        if h and lib is not None:  # at interpreter exit the module may be gone
+            lib.gfd_preconditioner_destroy(h)
             self.handle = None
 
     def __call__(self, residuals, kpt=None):

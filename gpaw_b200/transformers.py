@@ -78,8 +78,9 @@ class _Transformer:
 
     def __del__(self):
         h = getattr(self, 'transformer', None)
-        if h:
-            _lib.lib.gfd_transformer_destroy(h)
+        lib = getattr(_lib, 'lib', None) if _lib is not None else None
+        if h and lib is not None:  # at interpreter exit the module may be gone
+            lib.gfd_transformer_destroy(h)
             self.transformer = None
 
     def apply(self, input, output, phases=None):

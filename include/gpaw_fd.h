@@ -270,7 +270,17 @@ GFD_API int gfd_poisson_result(const gfd_poisson* ps, int* niter, double* error)
 typedef struct gfd_poisson_batch gfd_poisson_batch;
 GFD_API int gfd_poisson_batch_create(int nsolvers, gfd_poisson* const* solvers,
                                      gfd_poisson_batch** batch);
+/* The same with flags: GFD_BATCH_NO_GROUPS runs every solver as its own
+ * graph branch (no grouped launches).  Grouping pays for one large batch of
+ * small grids; when many batches are in flight at once, as in a serving
+ * loop, plain branches overlap better. */
+#define GFD_BATCH_NO_GROUPS 1
+GFD_API int gfd_poisson_batch_create_ex(int nsolvers, gfd_poisson* const* solvers, int flags,
+                                        gfd_poisson_batch** batch);
 GFD_API int gfd_poisson_batch_destroy(gfd_poisson_batch* batch);
+/* phis[i] = rhos[i] = NULL leaves slot i unused in this launch: its solver
+ * runs no V-cycle and its result reads as refused (GFD_EUNSUPPORTED), so a
+ * batch captured once can serve fewer requests than it has slots. */
 GFD_API int gfd_poisson_batch_solve_async(gfd_poisson_batch* batch, double* const* phis,
                                           const double* const* rhos, double eps, double maxcharge,
                                           int maxiter, void* stream);

@@ -171,6 +171,29 @@ def test_grouped_batch_charged_and_maxiter(cuda):
         assert s.niter == 2
 
 
+@pytest.mark.parametrize('group', [True, False])
+def test_batch_unused_slots(cuda, group):
+    """A batch captured once serves fewer requests than it has slots: unused
+    slots (None) run nothing, and the used ones give the results alone."""
+    import torch
+    from gpaw_b200.serving import PoissonBatch
+    sizes = [32, 32, 32, 32]
+    _, solvers, rhos = make_batch(cuda, sizes, seed=610)
+    batch = PoissonBatch(solvers, group=group)
+    assert batch.grouped == (4 if group else 0)
+    for used in ([0, 2], [3], [0, 1, 2, 3]):
+        phis = [torch.zeros_like(r) if i in used else None for i, r in enumerate(rhos)]
+        res = batch.solve(phis, [r if i in used else None for i, r in enumerate(rhos)])
+        for i in range(4):
+            if i not in used:
+                assert res[i] is None
+                continue
+            phi, n = solve_alone(cuda, 32, rhos[i])
+            assert res[i][0] == n and torch.equal(phi, phis[i])
+    with pytest.raises(ValueError):
+        batch.solve([None] * 4, [None] * 4)
+
+
 def test_mixed_precision_batch_uses_branches(cuda):
     import torch
     sizes = [24, 32]
@@ -191,16 +214,16 @@ def test_server_alone_vs_mix(cuda, precision):
     rhos = [pair_density(grid_for(N, H, device=cuda), 7 + i) for i, N in enumerate(sizes)]
     torch.cuda.synchronize()
 
-    def serve(max_inflight, arrivals):
+    def serve(max_inflight, arrivals, slots=8):
         srv = PoissonServer(H, precision=precision, max_inflight=max_inflight, nstreams=8,
-                            device=cuda, keep_results=True)
+                            device=cuda, keep_results=True, slots=slots)
         reqs = [Request(i, N, arrivals[i], rhos[i]) for i, N in enumerate(sizes)]
         stats = srv.run(reqs)
         torch.cuda.synchronize()
         return reqs, stats
 
     mix, s_mix = serve(8, [0.0] * len(sizes))               # all at once, overlapping
-    alone, s_alone = serve(1, [0.0] * len(sizes))           # one at a time
+    alone, s_alone = serve(1, [0.0] * len(sizes), slots=1)  # one at a time
     staggered, _ = serve(4, [0.002 * i for i in range(len(sizes))])  # arriving over time
     assert s_mix['completed'] == len(sizes) and s_alone['completed'] == len(sizes)
     for a, b, c in zip(mix, alone, staggered):
