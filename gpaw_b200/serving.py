@@ -17,7 +17,7 @@ PoissonServer(...)
     `max_inflight` launches are in flight, the waiting requests of each size,
     oldest size first, take a pod (a single solver when one request waits,
     a batch pod when more do; a new pod within the device-memory budget if
-    none is free), fill its slots and launch it on the next stream,
+    none is free and the GPU is idle or the size has none yet), fill its slots and launch it on the next stream,
     overlapping the launches already on the GPU; unused slots run nothing.
     Completions are found by polling the oldest launch of each stream, and
     each pod returns to its pool.  Latency is completion minus arrival.
@@ -154,6 +154,7 @@ class PoissonServer:
         self.device = torch.device(device) if device is not None else torch.device('cuda')
         self.streams = [torch.cuda.Stream(self.device) for _ in range(nstreams)]
         self.free = collections.defaultdict(list)   # (N, slots) -> [_Pod]
+        self.npods = collections.defaultdict(int)   # N -> pods created
         self.used_bytes = 0
         self.keep_results = keep_results
         self.rejected = 0
@@ -211,17 +212,25 @@ class PoissonServer:
                     self._launch(pod, [Request(-1, N, 0.0, z)], stream)
                     stream.synchronize()
                     self.free[N, k].append(pod)
+                    self.npods[N] += 1
 
-    def _acquire(self, N, waiting):
+    def _acquire(self, N, waiting, busy):
         """A pod for `waiting` requests of size N: a single solver for one, a
-        pod of `slots` for more (whichever is free, preferring that one), or
-        a new one within the memory budget; None if none can be had."""
+        pod of `slots` for more (whichever is free, preferring that one).
+        A new pod (within the memory budget) only when the GPU is idle
+        (busy = 0) or no pod of this size exists: its allocation would stall
+        the launches in flight.  None if none can be had now."""
         want = 1 if waiting == 1 or self.slots == 1 else self.slots
         other = self.slots if want == 1 else 1
         for k in (want, other):
             if self.free[N, k]:
                 return self.free[N, k].pop()
-        return self._new_pod(N, want)
+        if busy and self.npods[N]:
+            return None
+        pod = self._new_pod(N, want)
+        if pod is not None:
+            self.npods[N] += 1
+        return pod
 
     # -- serving loop ----------------------------------------------------------
     def run(self, requests):
@@ -265,7 +274,7 @@ class PoissonServer:
             for N in sorted((n for n in queues if queues[n]), key=lambda n: queues[n][0].arrival):
                 q = queues[N]
                 while q and ninflight < self.max_inflight:
-                    pod = self._acquire(N, len(q))
+                    pod = self._acquire(N, len(q), ninflight)
                     if pod is None:
                         if not ninflight:  # cannot ever fit
                             req = q.popleft()
