@@ -42,13 +42,14 @@ GFD_TUNE_POTENTIAL = 3
 
 class TunePlan(ctypes.Structure):
     """gfd_tune_plan: form 0 one thread per point / 1 marching kernel, the
-    marching tile (0: 32 columns, 1: 16, 2: 8), the axis-0 split target in
-    CTAs per SM and the measured microseconds per launch."""
+    marching tile (0: 32 columns, 1: 16, 2: 8, 3: 32 columns by 8 rows), the
+    axis-0 split target in CTAs per SM and the measured microseconds per
+    launch."""
     _fields_ = [('form', ctypes.c_int), ('tile', ctypes.c_int), ('ctas_per_sm', ctypes.c_int),
                 ('us', ctypes.c_double)]
 
     def as_dict(self):
-        return {'form': ('direct', 'march')[self.form], 'tile': (32, 16, 8)[self.tile],
+        return {'form': ('direct', 'march')[self.form], 'tile': (32, 16, 8, '32x8')[self.tile],
                 'ctas_per_sm': self.ctas_per_sm, 'us': self.us}
 
 # Every function the header declares: name -> (restype, argtypes).

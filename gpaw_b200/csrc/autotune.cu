@@ -59,7 +59,7 @@ int per_mask(const int per[3]) { return (per[0] ? 1 : 0) | (per[1] ? 2 : 0) | (p
 
 bool plan_valid(const TunePlan& p) {
   return (p.path == PLAN_DIRECT || p.path == PLAN_MARCH) && p.tile >= TILE_WIDE &&
-         p.tile <= TILE_NARROW && p.cps >= 1 && p.cps <= 64;
+         p.tile <= TILE_SHORT && p.cps >= 1 && p.cps <= 64;
 }
 
 int load_file(const char* path);
@@ -253,6 +253,7 @@ extern "C" int gfd_autotune_operator(gfd_operator* op, int dtype, int mode, cons
                                                  : OP_APPLY;
   std::vector<int> tiles = {TILE_WIDE};
   if (op->R <= 2) tiles = {TILE_WIDE, TILE_MID, TILE_NARROW};
+  if (dtype == GFD_COMPLEX128 && imode == OP_APPLY && op->R <= 4) tiles.push_back(TILE_SHORT);
   const std::vector<TunePlan> cands = march_candidates(tiles);
   const double* ph = dtype_is_complex(dtype) ? phase_cd : nullptr;
   TunePlan pick;

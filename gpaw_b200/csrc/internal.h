@@ -54,7 +54,9 @@ int num_sms();
 // and band-count class, the kernel form and the axis-0 split.  Launches use
 // the cached plan when there is one and the built-in rules otherwise.
 // ---------------------------------------------------------------------------
-enum { TILE_WIDE = 0, TILE_MID = 1, TILE_NARROW = 2 };  // marching tiles 32 / 16 / 8 wide
+// Marching tiles 32 / 16 / 8 columns wide; TILE_SHORT: 32 columns by 8 rows
+// (complex128 apply up to radius 4 only: 128 threads, four CTAs per SM).
+enum { TILE_WIDE = 0, TILE_MID = 1, TILE_NARROW = 2, TILE_SHORT = 3 };
 enum { PLAN_DIRECT = 0, PLAN_MARCH = 1 };               // one thread per point / marching
 enum { TK_STAR = 0, TK_RESTRICT = 1, TK_INTERP = 2 };
 

@@ -119,8 +119,15 @@ constexpr size_t star_smem_bytes() {
 //    c0' = -(1-w) c0 / w, which equals (1-w) phi + w (rho - sum) / c0.
 //  * The source term of MODE_JACOBI / MODE_RESIDUAL travels in the same
 //    pipeline stages.
+// The short tile (32 x 4 threads, 2 rows each) is meant to run four CTAs
+// per SM (128 registers).
+template <int BZ, int TY, int VY>
+constexpr int star_min_ctas() {
+  return BZ == 32 && TY == 4 && VY == 2 ? 4 : 1;
+}
+
 template <class V, int R, int BZ, int TY, int VY, int S, int MODE>
-__global__ void __launch_bounds__(BZ * TY)
+__global__ void __launch_bounds__(BZ * TY, star_min_ctas<BZ, TY, VY>())
 star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__ rho,
             const StarParams<typename vt<V>::S> p) {
   pdl_enter();

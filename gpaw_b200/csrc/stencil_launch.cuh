@@ -30,6 +30,7 @@ inline TileDims tile_dims(int tile) {
   switch (tile) {
     case TILE_NARROW: return {8, 8, 64};
     case TILE_MID: return {16, 16, 128};
+    case TILE_SHORT: return {32, 8, 128};
     default: return {32, 16, 128};
   }
 }
@@ -116,10 +117,22 @@ int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t n
 // radii up to 3 only, which keeps the number of kernels in check.
 constexpr int kMaxComplexRelaxR = 3;
 
+// The short tile exists for complex128 apply up to radius 4 (beyond, its
+// 2R + 1 partial sums per row do not fit 128 registers).
+constexpr int kMaxShortR = 4;
 template <class V, int R, int MODE>
-int star_wide(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
+constexpr bool has_short_tile() {
+  return sizeof(V) >= 16 && MODE == MODE_APPLY && R <= kMaxShortR;
+}
+
+template <class V, int R, int MODE>
+int star_wide(const gfd_operator* op, int tile, const V* in, V* out, const V* rho, int64_t nin,
               const StarParams<typename vt<V>::S>& p, const LaunchGeom& g, double* partials,
               cudaStream_t s) {
+  if constexpr (has_short_tile<V, R, MODE>()) {
+    if (tile == TILE_SHORT)
+      return star_go<V, R, 32, 4, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+  }
   if constexpr (sizeof(V) >= 16 || R > 3)
     return star_go<V, R, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
   else
@@ -136,14 +149,14 @@ int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V
       return star_go<V, RR, 8, 8, 1, MODE>(op, in, out, rho, nin, p, g, partials, s);        \
     if (tile == TILE_MID)                                                                    \
       return star_go<V, RR, 16, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);       \
-    return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
+    return star_wide<V, RR, MODE>(op, tile, in, out, rho, nin, p, g, partials, s);
 #define GFD_STAR_WIDE(RR)                                                                    \
   case RR:                                                                                   \
     if constexpr (RR > kMaxComplexRelaxR && vt<V>::NC == 2 && MODE != MODE_APPLY &&          \
                   MODE != MODE_POTENTIAL)                                                    \
       return set_error(GFD_EUNSUPPORTED, "complex Jacobi/residual sweeps need radius <= 3"); \
     else                                                                                     \
-      return star_wide<V, RR, MODE>(op, in, out, rho, nin, p, g, partials, s);
+      return star_wide<V, RR, MODE>(op, tile, in, out, rho, nin, p, g, partials, s);
   switch (op->R) {
     GFD_STAR_SMALL(1)
     GFD_STAR_SMALL(2)
@@ -307,8 +320,16 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
       return star_tma_dispatch(op, vin, vout, nin, p, g, s);
     }
   }
-  // Radii above 2 have the wide tile only.
-  const int tile = tuned && op->R <= 2 ? plan.tile : pick_tile(op);
+  // Radii above 2 have the wide tile only (and the short one for complex128
+  // apply): any other plan tile falls back to the built-in choice, so the
+  // geometry always matches the kernel launched.
+  int tile = pick_tile(op);
+  if (tuned) {
+    if (plan.tile == TILE_SHORT)
+      tile = sizeof(V) >= 16 && mode == OP_APPLY && op->R <= kMaxShortR ? TILE_SHORT : tile;
+    else if (op->R <= 2)
+      tile = plan.tile;
+  }
   LaunchGeom g = star_geom(op, tile, nin, op->R, tuned ? plan.cps : 0);
   p.nxc = g.nxc;
   p.x_chunk = g.x_chunk;

@@ -323,7 +323,7 @@ GFD_API int gfd_poisson_batch_grouped(const gfd_poisson_batch* batch, int* group
 
 typedef struct gfd_tune_plan {
   int form;         /* 0: one thread per point; 1: marching kernel */
-  int tile;         /* marching tile: 0 32 columns, 1 16, 2 8 */
+  int tile;         /* marching tile: 0 32 columns, 1 16, 2 8, 3 32 columns x 8 rows */
   int ctas_per_sm;  /* axis-0 split target */
   double us;        /* measured time per launch, microseconds */
 } gfd_tune_plan;
