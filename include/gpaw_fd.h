@@ -107,7 +107,7 @@ GFD_API int gfd_operator_apply(gfd_operator* op, int dtype, const void* in, void
  * the reference.  GFD_RELAX_GS: the reference's lexicographic Gauss-Seidel
  * is a sequential sweep; it is replaced by multicolour Gauss-Seidel
  * ((i0+i1+i2) mod (range+1) colours, a valid colouring for axis-aligned
- * stencils), judged by the converged result, not by iterates.
+ * stencils), compared by the converged result, not by iterates.
  * Uses a device scratch array of one grid owned by the operator. */
 GFD_API int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method, void* func,
                        const void* source, int nrelax, double w, void* stream);
