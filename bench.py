@@ -193,6 +193,7 @@ class CpuStencil:
         self.a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
         self.ph = G.bloch_phases(gd, K_VEC)
         self.threads = os.cpu_count() or 1
+        self.isa = K.ISA
         self.nbands = nbands_sample
         self.bytes = BYTES_PER_POINT * nbands_sample * N ** 3
 
@@ -224,8 +225,8 @@ def run_reference_arm(args):
         cpu.step()
     total = time.perf_counter() - t0
     value = float(args.steps * cpu.bytes / total / 1e9)
-    sample = '%d of the %d bands per step (%s C path, %d threads)' % (
-        cpu.nbands, NBANDS, cpu.kind, cpu.threads)
+    sample = '%d of the %d bands per step (%s C path, %d threads, %s build)' % (
+        cpu.nbands, NBANDS, cpu.kind, cpu.threads, cpu.isa)
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'GB/s',
             'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': total / args.steps * 1e3, 'higher_is_better': True,
@@ -260,7 +261,7 @@ def poisson_rho(gd, ng, seed, wall=2.0):
     return rho - rho.mean()
 
 
-def poisson_bench(nsolves=8, tune=True):
+def poisson_bench(nsolves=8, tune=True, check=True):
     import torch
     from gpaw_b200.grid_descriptor import GridDescriptor
     from gpaw_b200.poisson import PoissonSolver
@@ -293,7 +294,30 @@ def poisson_bench(nsolves=8, tune=True):
                      'residual': float(ps.error), 'autotuned': bool(tune)}
     out['mixed_vs_fp64_speedup'] = out['mixed']['solves_per_s'] / out['fp64']['solves_per_s']
     out['mixed_max_abs_vs_fp64'] = float(np.abs(phis['mixed'] - phis['fp64']).max())
+    if check:
+        out['oracle'] = poisson_oracle_check(gd, rho_h, phis, out)
     return out, phis, rho_h, gd
+
+
+def poisson_oracle_check(gd, rho_h, phis, out):
+    """The same solve by the CPU oracle (the reference's V-cycle restated
+    over its C kernels): V-cycle count and max-abs error of the timed GPU
+    potentials against it."""
+    from oracle import geometry as G
+    from oracle import poisson as OP
+    og = G.Grid(gd.N_c, gd.cell_cv, gd.pbc_c)
+    ps = OP.PoissonSolver(3, 'J', 2e-10)
+    ps.set_grid_descriptor(og)
+    ps.initialize()
+    phi_o = np.zeros(tuple(og.n_c))
+    t0 = time.perf_counter()
+    n_o = ps.solve(phi_o, rho_h)
+    dt = time.perf_counter() - t0
+    return {'vcycles': int(n_o), 'residual': float(ps.errors[-1]), 'cpu_seconds': dt,
+            'fp64_vcycles_match': int(n_o) == out['fp64']['vcycles'],
+            'fp64_max_abs_vs_oracle': float(np.abs(phis['fp64'] - phi_o).max()),
+            'mixed_max_abs_vs_oracle': float(np.abs(phis['mixed'] - phi_o).max()),
+            'bars': {'fp64': 1e-10, 'mixed': 1e-9}}
 
 
 # ---------------------------------------------------------------------------
@@ -610,6 +634,20 @@ def preconditioner_bench(gd, lap, a, b, phase, steps):
             'speedup': unfused_ms / fused_ms}
 
 
+def headline_oracle_check(lap, a, b, phase):
+    """Max relative error (max |gpu - oracle| / max |oracle|) of the last
+    timed apply on the first, middle and last band against the oracle."""
+    from oracle import kernels as K
+    idx = sorted({0, a.shape[0] // 2, a.shape[0] - 1})
+    a_h = a[idx].cpu().numpy()
+    b_h = b[idx].cpu().numpy()
+    ref = K.fd_apply(lap.coef_p, lap.offset_pc, lap.gd.pbc_c, a_h, phase,
+                     nthreads=os.cpu_count() or 1)
+    err = float(np.abs(b_h - ref).max() / np.abs(ref).max())
+    return {'bands_checked': idx, 'max_rel_err_vs_oracle': err, 'bar': 1e-13,
+            'oracle': 'C restatement of c/bmgs/fd.c + c/bc.c (bit-equal to the reference C)'}
+
+
 # ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
@@ -692,6 +730,10 @@ def run_gpu_arm(args):
                'pinned_host_memory': pinned}
         del host_in, host_out, streamer
 
+    # The timed output, checked: three of this rank's bands against the
+    # oracle (the reference's stencil and Bloch halo restated in C).
+    check = headline_oracle_check(lap, a, b, phase) if not args.no_cpu else None
+
     ham = pcb = var = None
     if rank == 0 and world == 1 and not args.no_hamiltonian:
         ham = hamiltonian_bench(lap, a, b, phase, min(args.steps, 20))
@@ -712,6 +754,7 @@ def run_gpu_arm(args):
                                     if plan and plan['form'] == 'direct'
                                     else 'star_kernel<cplx<double>,R=3>')},
             'launch_plan': plan,
+            'check': check,
             'e2e': e2e,
             'gpu_launches': args.steps,
             'clocks': clocks.result()}
@@ -738,8 +781,8 @@ def run_gpu_arm(args):
         r, reps, dt = cpu.rate(args.cpu_seconds)
         line['cpu_baseline'] = {'value': r, 'unit': 'GB/s', 'cores': cpu.threads,
                                 'kind': cpu.kind,
-                                'sample': '16 of the 512 bands, %d passes in %.1f s'
-                                          % (reps, dt)}
+                                'sample': '16 of the 512 bands, %d passes in %.1f s '
+                                          '(%s build)' % (reps, dt, cpu.isa)}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

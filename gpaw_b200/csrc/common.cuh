@@ -111,13 +111,22 @@ __device__ __forceinline__ double sq(float v) { return double(v) * double(v); }
 // phase_cd[c][1]), 0 high halo (takes phase_cd[c][0]); the convention of
 // c/bc.c:234-249 where slab d is copied to the far side times phases[d].
 // ---------------------------------------------------------------------------
+// A tile that overhangs a short periodic axis asks for coordinates more than
+// one period away (u >= 2n, e.g. a 32-wide tile on a 16-point axis).  Only
+// outputs outside the domain use those cells, so any in-range index serves;
+// the coordinate is reduced modulo n so every load stays inside the array.
 __device__ __forceinline__ int wrap_axis(int u, int n, int periodic, int& side) {
   side = -1;
   if (u >= 0 && u < n) return u;
   if (!periodic) return -1;
-  if (u < 0) { side = 1; return u + n; }
+  if (u < 0) {
+    side = 1;
+    u += n;
+    return u >= 0 ? u : (u % n + n) % n;
+  }
   side = 0;
-  return u - n;
+  u -= n;
+  return u < n ? u : u % n;
 }
 
 // Phases for the three axes: ph[c][d], d = 0 high halo, 1 low halo.
@@ -145,6 +154,8 @@ __device__ __forceinline__ void pdl_enter() {
 }
 
 bool pdl_enabled();
+// Complex bands on the lane-pair stencil kernel (GFD_SPLIT=0 turns it off).
+bool split_enabled();
 // Largest grid (points over all bands) for the one-thread-per-point kernels.
 long long direct_max_points();
 // CTAs per SM the marching kernels aim for when they split axis 0 into

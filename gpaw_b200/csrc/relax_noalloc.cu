@@ -12,11 +12,14 @@
 // fixed scratch array compiled into the library instead.
 //
 // The scratch is a file-scope __device__ array of kNoAllocScratchBytes
-// (16 MiB: 2,097,152 float64 or 4,194,304 float32 grid points, enough for a
-// 127^3 float64 grid).  Every GPU on which the library is loaded holds it
-// until the process exits.  Host code must not pass the array's name to a
-// kernel (on the host it names a stand-in, not device memory); the device
-// address is looked up once per device with cudaGetSymbolAddress.
+// (16 MiB: up to 2,097,152 float64 points, a 128^3 grid, or 4,194,304
+// float32 points).  Every GPU on which the library is loaded holds it until
+// the process exits.  Host code must not pass the array's name to a kernel
+// (on the host it names a stand-in, not device memory); the device address
+// is looked up with cudaGetSymbolAddress, with the device current, on the
+// first call in each CUDA context of a device, and cached.  A context that
+// is destroyed and created again (cudaDeviceReset) gets a new lookup, since
+// the module, and with it the array, may then sit at another address.
 #include <mutex>
 #include <string>
 
@@ -29,10 +32,31 @@ constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 
 static __device__ __align__(256) unsigned char g_relax_scratch[kNoAllocScratchBytes];
 
-// Device address of g_relax_scratch on each device, set on the first call
-// made with that device current.
-static void* g_scratch_addr[64] = {nullptr};
+// Per device: the context the address was looked up in and the address.
+struct ScratchAddr {
+  void* ctx = nullptr;
+  void* addr = nullptr;
+};
+static ScratchAddr g_scratch_addr[64];
 static std::mutex g_scratch_mutex;
+
+// The current context (CUcontext, as void*) through the driver entry point,
+// so the library needs no link-time dependency on libcuda.
+typedef int (*CtxGetCurrentFn)(void**);
+static int current_context(void** ctx) {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  if (!fn) return set_error(GFD_ECUDA, "cuCtxGetCurrent is not available");
+  *ctx = nullptr;
+  if (fn(ctx) != 0 || !*ctx) return set_error(GFD_ECUDA, "no current CUDA context");
+  return GFD_OK;
+}
 
 static int scratch_for_current_device(void** out) {
   int dev = 0;
@@ -40,14 +64,22 @@ static int scratch_for_current_device(void** out) {
   if (st) return st;
   if (dev < 0 || dev >= 64) return set_error(GFD_EUNSUPPORTED, "device index out of range");
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
+  ScratchAddr& e = g_scratch_addr[dev];
+  void* ctx = nullptr;
+  // No current context yet (a first call before any other CUDA work on this
+  // thread) reads as "not cached": the lookup below makes the runtime bind
+  // the device's primary context, which is then recorded.
+  if (current_context(&ctx) != GFD_OK) ctx = nullptr;
+  if (!e.addr || !ctx || e.ctx != ctx) {
     void* p = nullptr;
     st = check_cuda(cudaGetSymbolAddress(&p, g_relax_scratch),
                     "cudaGetSymbolAddress(relaxation scratch)");
     if (st) return st;
-    g_scratch_addr[dev] = p;
+    if ((st = current_context(&ctx))) return st;
+    e.ctx = ctx;
+    e.addr = p;
   }
-  *out = g_scratch_addr[dev];
+  *out = e.addr;
   return GFD_OK;
 }
 

@@ -123,7 +123,9 @@ GFD_API int gfd_operator_relax(gfd_operator* op, int dtype, int relax_method, vo
  * most 2,097,152 float64 or 4,194,304 float32 points; larger grids return
  * GFD_EINVAL with a message.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before starting any stream capture.  All calls share
+ * make that first call before starting any stream capture.  After a device
+ * reset (cudaDeviceReset) the next call sees a new context and looks the
+ * address up again, so it too must come before any capture.  All calls share
  * the one array: calls that overlap on the GPU (on different streams, or
  * from different threads) race on it and must be serialised by the caller. */
 GFD_API int gfd_operator_relax_noalloc(gfd_operator* op, int dtype, int relax_method, void* func,
@@ -323,7 +325,8 @@ GFD_API int gfd_poisson_batch_grouped(const gfd_poisson_batch* batch, int* group
 
 typedef struct gfd_tune_plan {
   int form;         /* 0: one thread per point; 1: marching kernel */
-  int tile;         /* marching tile: 0 32 columns, 1 16, 2 8, 3 32 columns x 8 rows */
+  int tile;         /* marching tile: 0 32 columns, 1 16, 2 8, 3 32 columns x 8 rows,
+                       4 complex bands with re / im on lane pairs (radius <= 3) */
   int ctas_per_sm;  /* axis-0 split target */
   double us;        /* measured time per launch, microseconds */
 } gfd_tune_plan;

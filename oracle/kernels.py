@@ -14,8 +14,35 @@ import numpy as np
 from . import geometry
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-PORT_PATH = os.path.join(_HERE, 'liboracle.so')
-REF_PATH = os.path.join(_HERE, '_ref', 'libgpawref.so')
+
+
+def _host_has_avx512():
+    """True when the CPU offers the x86-64-v4 feature set (AVX-512 F, BW,
+    CD, DQ, VL)."""
+    try:
+        with open('/proc/cpuinfo') as f:
+            for line in f:
+                if line.startswith('flags'):
+                    flags = set(line.split(':', 1)[1].split())
+                    return {'avx512f', 'avx512bw', 'avx512cd', 'avx512dq',
+                            'avx512vl'} <= flags
+    except OSError:
+        pass
+    return False
+
+
+def _variant(path):
+    """The x86-64-v4 build of a library where the host supports it and it
+    was built, else the x86-64-v3 one."""
+    v4 = path[:-3] + '_v4.so'
+    if _host_has_avx512() and os.path.exists(v4):
+        return v4
+    return path
+
+
+PORT_PATH = _variant(os.path.join(_HERE, 'liboracle.so'))
+REF_PATH = _variant(os.path.join(_HERE, '_ref', 'libgpawref.so'))
+ISA = 'x86-64-v4' if PORT_PATH.endswith('_v4.so') else 'x86-64-v3'
 
 _libs = {}
 
