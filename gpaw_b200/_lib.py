@@ -21,6 +21,9 @@ GFD_ENOCONV = 3
 GFD_ETIMEOUT = 4
 GFD_ECUDA = 5
 GFD_EUNSUPPORTED = 6
+GFD_ENEEDGAUSS = 7
+
+GFD_SOLVE_ZERO_INITIAL_PHI = 1
 
 GFD_FLOAT64 = 0
 GFD_COMPLEX128 = 1
@@ -42,14 +45,17 @@ GFD_TUNE_POTENTIAL = 3
 
 class TunePlan(ctypes.Structure):
     """gfd_tune_plan: form 0 one thread per point / 1 marching kernel, the
-    marching tile (0: 32 columns, 1: 16, 2: 8, 3: 32 columns by 8 rows), the
+    marching tile (0: 32 columns, 1: 16, 2: 8, 3: 32 columns by 8 rows, 4: complex
+    bands with the real and imaginary parts on lane pairs, 5: the same for
+    complex128 on full rows staged by TMA), the
     axis-0 split target in CTAs per SM and the measured microseconds per
     launch."""
     _fields_ = [('form', ctypes.c_int), ('tile', ctypes.c_int), ('ctas_per_sm', ctypes.c_int),
                 ('us', ctypes.c_double)]
 
     def as_dict(self):
-        return {'form': ('direct', 'march')[self.form], 'tile': (32, 16, 8, '32x8')[self.tile],
+        return {'form': ('direct', 'march')[self.form],
+                'tile': (32, 16, 8, '32x8', 'split', 'tma-split')[self.tile],
                 'ctas_per_sm': self.ctas_per_sm, 'us': self.us}
 
 # Every function the header declares: name -> (restype, argtypes).
@@ -70,6 +76,8 @@ SIGNATURES = {
                                                   ctypes.c_int, ctypes.c_double, _vp]),
     'gfd_operator_get_diagonal_element': (ctypes.c_int, [_vp, _dp]),
     'gfd_device_errors': (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    'gfd_wait_selftest': (ctypes.c_int, [ctypes.c_longlong]),
+    'gfd_test_fail_alloc': (ctypes.c_int, [ctypes.c_longlong]),
     'gfd_density_interpolate': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, _vp]),
     'gfd_poisson_set_rhs_operator': (ctypes.c_int, [_vp, _vp]),
@@ -92,6 +100,12 @@ SIGNATURES = {
     'gfd_poisson_destroy': (ctypes.c_int, [_vp]),
     'gfd_poisson_solve': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, _ip, _dp, _vp]),
+    'gfd_poisson_solve_ex': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp,
+                                            _vp]),
+    'gfd_poisson_load_gauss': (ctypes.c_int, [_vp, _dp, _i64p, _dp, ctypes.c_double, _vp]),
+    'gfd_poisson_set_madelung': (ctypes.c_int, [_vp, ctypes.c_double]),
+    'gfd_madelung': (ctypes.c_int, [_dp, _dp]),
     'gfd_poisson_solve_async': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, _vp]),
     'gfd_poisson_result': (ctypes.c_int, [_vp, _ip, _dp]),
@@ -156,7 +170,7 @@ def check(status, what=''):
         raise MemoryError(msg)
     if status == GFD_ENOCONV:
         raise PoissonConvergenceError(msg)
-    if status == GFD_EUNSUPPORTED:
+    if status in (GFD_EUNSUPPORTED, GFD_ENEEDGAUSS):
         raise NotImplementedError(msg)
     raise RuntimeError('%s (status %d)' % (msg, status))
 

@@ -31,6 +31,30 @@ int check_cuda(cudaError_t e, const char* what) {
 
 int check_launch(const char* what) { return check_cuda(cudaGetLastError(), what); }
 
+// Device allocations of the library go through dev_malloc.  A host-side
+// fault hook (gfd_test_fail_alloc) can make the n-th next allocation fail as
+// cudaMalloc would when memory is exhausted, without touching the device.
+static std::mutex g_alloc_mu;
+static long long g_fail_countdown = 0;  // 0: no failure planned
+
+int dev_malloc(void** p, size_t bytes, const char* what) {
+  {
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    if (g_fail_countdown > 0 && --g_fail_countdown == 0) {
+      *p = nullptr;
+      return set_error(GFD_ENOMEM, std::string(what) + ": out of memory (planned failure)");
+    }
+  }
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_error(e == cudaErrorMemoryAllocation ? GFD_ENOMEM : GFD_ECUDA,
+                     std::string(what) + ": " + cudaGetErrorString(e));
+  }
+  return GFD_OK;
+}
+
 // Programmatic dependent launch is opt-in (GFD_PDL=1): in the Poisson solve
 // graph, whose kernels are short, starting dependents early cost 3% of
 // solves/s; the streaming kernels neither gain nor lose.
@@ -51,6 +75,14 @@ long long direct_max_points() {
     return e ? atoll(e) : 300000LL;
   }();
   return v;
+}
+
+bool split_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("GFD_SPLIT");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 int march_ctas_per_sm() {
@@ -192,6 +224,13 @@ int convert_launch(int ydtype, void* y, int xdtype, const void* x, int64_t n, cu
 }  // namespace gfd
 
 using namespace gfd;
+
+extern "C" int gfd_test_fail_alloc(long long n) {
+  if (n < 0) return set_error(GFD_EINVAL, "allocation count must be >= 0");
+  std::lock_guard<std::mutex> lock(g_alloc_mu);
+  g_fail_countdown = n;
+  return GFD_OK;
+}
 
 extern "C" size_t gfd_last_error(char* buf, size_t len) {
   const std::string& m = g_last_error;

@@ -129,6 +129,20 @@ __device__ __forceinline__ int wrap_axis(int u, int n, int periodic, int& side) 
   return u < n ? u : u % n;
 }
 
+// The same for a plane index of a marching kernel, which lies in
+// [-R, n + R) with n >= R on a periodic axis: one wrap at most.
+__device__ __forceinline__ int wrap_plane(int u, int n, int periodic, int& side) {
+  side = -1;
+  if (u >= 0 && u < n) return u;
+  if (!periodic) return -1;
+  if (u < 0) {
+    side = 1;
+    return u + n;
+  }
+  side = 0;
+  return u - n;
+}
+
 // Phases for the three axes: ph[c][d], d = 0 high halo, 1 low halo.
 template <class S>
 struct Phases {
@@ -184,6 +198,9 @@ inline cudaError_t launch_k(void (*kern)(P...), dim3 grid, dim3 block, size_t sm
 // Host-side error plumbing.
 // ---------------------------------------------------------------------------
 int set_error(int code, const std::string& msg);
+// cudaMalloc with the library's status codes (GFD_ENOMEM on exhaustion) and
+// the planned-failure hook of gfd_test_fail_alloc.
+int dev_malloc(void** p, size_t bytes, const char* what);
 int check_cuda(cudaError_t e, const char* what);
 int check_launch(const char* what);
 

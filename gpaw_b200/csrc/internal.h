@@ -56,7 +56,18 @@ int num_sms();
 // ---------------------------------------------------------------------------
 // Marching tiles 32 / 16 / 8 columns wide; TILE_SHORT: 32 columns by 8 rows
 // (complex128 apply up to radius 4 only: 128 threads, four CTAs per SM).
-enum { TILE_WIDE = 0, TILE_MID = 1, TILE_NARROW = 2, TILE_SHORT = 3 };
+// TILE_SPLIT: complex bands, radius <= 3, real and imaginary parts on lane
+// pairs (star_split_kernel): 32 columns by 16 rows, 128 threads.
+// TILE_TMASPLIT: complex128, radius <= 3, the same lane pairs on full-row
+// tiles of 8 rows staged by TMA (star_tmasplit_kernel).
+enum {
+  TILE_WIDE = 0,
+  TILE_MID = 1,
+  TILE_NARROW = 2,
+  TILE_SHORT = 3,
+  TILE_SPLIT = 4,
+  TILE_TMASPLIT = 5
+};
 enum { PLAN_DIRECT = 0, PLAN_MARCH = 1 };               // one thread per point / marching
 enum { TK_STAR = 0, TK_RESTRICT = 1, TK_INTERP = 2 };
 

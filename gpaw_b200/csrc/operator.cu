@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "stencil_launch.cuh"
+#include "stencil_tmasplit.cuh"
 
 GFD_DECLARE_STENCIL_ENTRY(f64)
 GFD_DECLARE_STENCIL_ENTRY(f32)
@@ -88,12 +89,8 @@ static int ensure_scratch(gfd_operator* op, size_t bytes) {
     op->scratch = nullptr;
     op->scratch_bytes = 0;
   }
-  cudaError_t e = cudaMalloc(&op->scratch, bytes);
-  if (e != cudaSuccess) {
-    op->scratch = nullptr;
-    cudaGetLastError();
-    return set_error(GFD_ENOMEM, "cudaMalloc of relaxation scratch failed");
-  }
+  int st = dev_malloc(&op->scratch, bytes, "cudaMalloc of relaxation scratch");
+  if (st) return st;
   op->scratch_bytes = bytes;
   cudaGetDevice(&op->device);
   return GFD_OK;
@@ -105,6 +102,17 @@ static int ensure_scratch(gfd_operator* op, size_t bytes) {
 // ---------------------------------------------------------------------------
 // Set by a kernel whose bounded mbarrier wait expired.
 __device__ int g_star_err = 0;
+
+// The TMA-staged lane-pair kernel is the default for complex128 bands it
+// can take; GFD_TMASPLIT=0 in the environment keeps them on the cp.async
+// kernels (for comparisons).
+bool tmasplit_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("GFD_TMASPLIT");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 
 // Opt-in (GFD_STAR_TMA=1): on the 96^3 x 512-band complex128 workload the
 // TMA-fed kernel measured 2.6 TB/s against 3.7 TB/s for star_kernel.
@@ -174,6 +182,59 @@ static int encode_one(CUtensorMap* m, const void* base, const gfd_operator* op, 
   return GFD_OK;
 }
 
+// Maps of star_tmasplit_kernel (stencil_tmasplit.cuh).  Bands as doubles
+// (2, n2, n1, n0, nb) with element stride 2 on the column axis, so one box
+// takes every second column: box (2, 2 pw, rows, 1, 1) stages pw values of
+// one column parity for `rows` rows.
+static int encode_parity(CUtensorMap* m, const void* base, const gfd_operator* op, int64_t nb,
+                         int pw, int rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(GFD_ECUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t row = cuuint64_t(op->n[2]) * 16;
+  cuuint64_t dims[5] = {2, cuuint64_t(op->n[2]), cuuint64_t(op->n[1]), cuuint64_t(op->n[0]),
+                        cuuint64_t(nb)};
+  cuuint64_t strides[4] = {16, row, row * op->n[1], row * op->n[1] * op->n[0]};
+  cuuint32_t box[5] = {2, cuuint32_t(2 * pw), cuuint32_t(rows), 1, 1};
+  cuuint32_t estr[5] = {1, 2, 1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(GFD_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  return GFD_OK;
+}
+
+int encode_ts_maps(TsMaps* maps, const void* in, const void* rho, const void* pot,
+                   const gfd_operator* op, int64_t nb, int R, int ng) {
+  const int re = (R + 1) & ~1;
+  const int pw = ts_pw(ng, re), sy = kTsBY + 2 * R;
+  int st;
+  if ((st = encode_parity(&maps->rows_full, in, op, nb, pw, sy))) return st;
+  if ((st = encode_parity(&maps->rows_main, in, op, nb, pw, sy - R))) return st;
+  if ((st = encode_parity(&maps->rows_own, in, op, nb, pw, kTsBY))) return st;
+  if ((st = encode_parity(&maps->rows_halo, in, op, nb, pw, R))) return st;
+  std::memset(&maps->rho, 0, sizeof maps->rho);
+  std::memset(&maps->pot, 0, sizeof maps->pot);
+  if (rho && (st = encode_parity(&maps->rho, rho, op, nb, ts_pwr(ng), kTsBY))) return st;
+  if (pot) {
+    // The potential: one real grid (n2, n1, n0), box (32 ng, BY, 1).
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return set_error(GFD_ECUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t row = cuuint64_t(op->n[2]) * 8;
+    cuuint64_t dims[3] = {cuuint64_t(op->n[2]), cuuint64_t(op->n[1]), cuuint64_t(op->n[0])};
+    cuuint64_t strides[2] = {row, row * op->n[1]};
+    cuuint32_t box[3] = {cuuint32_t(32 * ng), cuuint32_t(kTsBY), 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(&maps->pot, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(pot), dims,
+                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return set_error(GFD_ECUDA,
+                       "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  }
+  return GFD_OK;
+}
+
 int encode_tma_maps(TmaMaps* maps, const void* base, const gfd_operator* op, int64_t nb, int R,
                     int by) {
   int st;
@@ -184,7 +245,40 @@ int encode_tma_maps(TmaMaps* maps, const void* base, const gfd_operator* op, int
 
 }  // namespace gfd
 
+namespace gfd {
+// A wait that nothing completes: thread 0 initialises an mbarrier nobody
+// arrives on, every thread waits on its first phase with the kernels'
+// bounded wait (limit max_cycles) and, when the wait runs out, the kernel
+// sets the device error flag exactly as the stencil kernels do.  No copy is
+// in flight, so the early exit leaves nothing behind.
+__global__ void wait_probe_kernel(int* err, long long max_cycles) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(&bar, 0u, &abort_flag, max_cycles)) {
+    abort_flag = 1;
+    if (threadIdx.x == 0) atomicExch(err, 1);
+  }
+}
+}  // namespace gfd
+
 using namespace gfd;
+
+extern "C" int gfd_wait_selftest(long long max_cycles) {
+  if (max_cycles < 1 || max_cycles > kSpinCycles)
+    return set_error(GFD_EINVAL, "wait limit out of range");
+  int* err = star_error_flag();
+  if (!err) return GFD_ECUDA;
+  wait_probe_kernel<<<1, 64>>>(err, max_cycles);
+  int st = check_launch("wait_probe_kernel");
+  if (st) return st;
+  return check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize(wait probe)");
+}
 
 extern "C" int gfd_device_errors(int* flags) {
   if (!flags) return set_error(GFD_EINVAL, "null argument");

@@ -38,15 +38,43 @@
 
 namespace {
 
+// The branch of PoissonSolver.solve (gpaw/poisson.py:124-191), from the
+// integral of rho (c->charge, reduced just before):
+//   |q| <= maxcharge      neutral: source rho - background;
+//   charged, periodic     source rho - background, phi shifted by q madelung;
+//   charged, non-periodic the monopole (the integral of rho) goes on the
+//                         L = 0 Gaussian: source rho - gq g, no background,
+//                         phi shifted by gq v, gq = charge / sqrt(4 pi);
+//   charged, mixed        refused (NotImplementedError in the reference).
 __global__ void prep_kernel(SolveCtrl* c, double npoints, double dv,
                             cudaGraphConditionalHandle loop, int in_graph) {
   gfd::pdl_enter();
   c->bg = c->charge / dv / npoints;
+  c->gq = 0.0;
+  c->shift = 0.0;
   const double q = isnan(c->charge_arg) ? c->charge : c->charge_arg;
-  c->status = fabs(q) > c->maxcharge ? GFD_EUNSUPPORTED : GFD_OK;
+  int status = GFD_OK;
+  if (c->skip) {
+    status = GFD_EUNSUPPORTED;
+  } else if (fabs(q) > c->maxcharge) {
+    if (c->bc_kind == kBcPeriodic) {
+      if (isnan(c->madelung)) status = GFD_EUNSUPPORTED;
+      else c->shift = q * c->madelung;
+    } else if (c->bc_kind == kBcNone) {
+      if (!c->rho_gauss || !c->phi_gauss) {
+        status = GFD_ENEEDGAUSS;
+      } else {
+        c->gq = c->charge * 0.28209479177387814;  // 1 / sqrt(4 pi)
+        c->bg = 0.0;
+      }
+    } else {
+      status = GFD_EUNSUPPORTED;
+    }
+  }
+  c->status = status;
   c->niter = 0;
   c->err = 0.0;
-  if (c->status != GFD_OK && in_graph) cudaGraphSetConditional(loop, 0);
+  if (status != GFD_OK && in_graph) cudaGraphSetConditional(loop, 0);
 }
 
 // One V-cycle done: count it and decide whether to run another
@@ -58,22 +86,79 @@ __global__ void check_kernel(SolveCtrl* c, cudaGraphConditionalHandle loop, int 
   if (in_graph) cudaGraphSetConditional(loop, (c->err > c->eps && n < c->maxiter) ? 1u : 0u);
 }
 
-// y = x - bg (background removal), bg read from the controls.
-__global__ void __launch_bounds__(256) sub_bg_kernel(double* y, const double* x,
+// Level-0 source y = x - bg - gq g (background removal, or the Gaussian of
+// the charged non-periodic branch) and, in the charged branches, the initial
+// guess phi - shift - gq v (phi = 0 with zero_initial_phi); the controls
+// hold the branch.
+__global__ void __launch_bounds__(256) source_kernel(double* y, const double* x, double* phi,
                                                      const SolveCtrl* c, long long n) {
   gfd::pdl_enter();
-  const double bg = c->bg;
-  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
-    y[i] = x[i] - bg;
+  const double bg = c->bg, gq = c->gq, shift = c->shift;
+  const bool charged = c->status == GFD_OK && (gq != 0.0 || shift != 0.0);
+  const bool zero = charged && c->zero_init;
+  const double* g = c->rho_gauss;
+  const double* v = c->phi_gauss;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    y[i] = gq != 0.0 ? x[i] - bg - gq * g[i] : x[i] - bg;
+    if (charged) phi[i] = zero ? 0.0 : (gq != 0.0 ? phi[i] - gq * v[i] : phi[i] - shift);
+  }
 }
 
-// phi -= sum / n (zero mean potential in fully periodic systems).
+// phi -= sum / n (zero mean potential in fully periodic systems), then
+// + the charged periodic branch's shift (gpaw/poisson.py:157, 212-216).
 __global__ void __launch_bounds__(256) sub_mean_kernel(double* phi, const SolveCtrl* c,
                                                        long long n) {
   gfd::pdl_enter();
-  const double m = c->sum / double(n);
+  const double m = c->sum / double(n) - c->shift;
   for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
     phi[i] -= m;
+}
+
+// Result to the caller: out = phi + gq v (the Gaussian's potential back on
+// in the charged non-periodic branch, gpaw/poisson.py:185-186).
+__global__ void __launch_bounds__(256) finish_kernel(double* out, const double* phi,
+                                                     const SolveCtrl* c, long long n) {
+  gfd::pdl_enter();
+  const double gq = c->status == GFD_OK ? c->gq : 0.0;
+  const double* v = c->phi_gauss;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+    out[i] = gq != 0.0 ? phi[i] + gq * v[i] : phi[i];
+}
+
+// The L = 0 Gaussian and its potential at every level-0 point
+// (gpaw/utilities/gauss.py:22, 35, 67-82; coordinates of
+// gpaw/utilities/tools.py:92-118): r_v = sum_c (i_c + beg_c) h_cv - center_v,
+// r^2 clamped to 1e-12, g = sqrt(4 a^3) / pi exp(-a r^2),
+// v = 2 sqrt(pi) erf(sqrt(a) r) / r.
+struct GaussGeom {
+  double h[9];
+  double center[3];
+  int beg[3];
+  int n[3];
+  double a;
+};
+__global__ void __launch_bounds__(256) gauss_kernel(double* g, double* v, const GaussGeom geo,
+                                                    long long total) {
+  gfd::pdl_enter();
+  const double norm = sqrt(4.0 * geo.a * geo.a * geo.a) / 3.141592653589793;
+  const double sa = sqrt(geo.a);
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < total;
+       i += (long long)gridDim.x * 256) {
+    const long long plane = (long long)geo.n[1] * geo.n[2];
+    const int i0 = int(i / plane);
+    const int r1 = int(i - i0 * plane);
+    const int i1 = r1 / geo.n[2], i2 = r1 - i1 * geo.n[2];
+    const double c0 = i0 + geo.beg[0], c1 = i1 + geo.beg[1], c2 = i2 + geo.beg[2];
+    double r2 = 0.0;
+    for (int d = 0; d < 3; d++) {
+      const double x = c0 * geo.h[d] + c1 * geo.h[3 + d] + c2 * geo.h[6 + d] - geo.center[d];
+      r2 += x * x;
+    }
+    if (r2 < 1e-12) r2 = 1e-12;
+    const double r = sqrt(r2);
+    g[i] = norm * exp(-geo.a * r2);
+    v[i] = 2.0 * 1.7724538509055159 * erf(sa * r) / r;
+  }
 }
 
 }  // namespace
@@ -169,16 +254,19 @@ static int iterate2(gfd_poisson* ps, int l, bool final_norm, cudaStream_t s,
   return GFD_OK;
 }
 
-// Level-0 source: rho_in - background (gpaw/poisson.py:128-138) and, for
-// the Mehrstellen form, B applied to it (gpaw/poisson.py:196-199).
+// Level-0 source: rho_in - background (gpaw/poisson.py:128-138), or the
+// charged branches' source and initial guess (source_kernel), and, for the
+// Mehrstellen form, B applied to it (gpaw/poisson.py:196-199).
 static int rhs_launch(gfd_poisson* ps, cudaStream_t s) {
   Level& L0 = ps->L[0];
   const int64_t n0 = L0.n;
   const bool fp64 = ps->precision == GFD_POISSON_FP64;
   double* rho0 = fp64 ? static_cast<double*>(L0.rho) : ps->rho64;
   double* dst = ps->B ? (fp64 ? static_cast<double*>(L0.res) : ps->r64) : rho0;
-  launch_k(sub_bg_kernel, grid_for(n0), 256, 0, s, dst, ps->rho_in, ps->dctrl, (long long)n0);
-  int st = check_launch("sub_bg_kernel");
+  double* phi_int = fp64 ? static_cast<double*>(L0.phi[0]) : ps->phi64;
+  launch_k(source_kernel, grid_for(n0), 256, 0, s, dst, ps->rho_in, phi_int, ps->dctrl,
+           (long long)n0);
+  int st = check_launch("source_kernel");
   if (st || !ps->B) return st;
   return op_launch(ps->B, GFD_FLOAT64, OP_APPLY, dst, rho0, nullptr, 1, nullptr, 0.0, nullptr, s);
 }
@@ -413,6 +501,21 @@ static int build_graph(gfd_poisson* ps) {
   return build_multi_graph(one, 1, &ps->graph, &ps->exec);
 }
 
+// Host-written part of the controls for one solve.
+static void set_inputs(gfd_poisson* ps, SolveCtrl* h, double charge, double eps,
+                       double maxcharge, int maxiter) {
+  h->eps = eps;
+  h->maxcharge = maxcharge;
+  h->charge_arg = charge;
+  h->maxiter = maxiter;
+  h->zero_init = ps->zero_init;
+  h->rho_gauss = ps->rho_gauss;
+  h->phi_gauss = ps->phi_gauss;
+  h->madelung = ps->madelung;
+  h->bc_kind = ps->bc_kind;
+  h->skip = 0;
+}
+
 // Copy-in of the controls, rho and phi (before a graph launch) and copy-out
 // of phi and the controls (after it); the results are read by
 // gfd_poisson_result once the stream has reached that point.
@@ -422,10 +525,7 @@ static int stage_in(gfd_poisson* ps, double* phi, const double* rho, double char
   double* phi_int = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
                                                       : ps->phi64;
   SolveCtrl* h = ps->hctrl;
-  h->eps = eps;
-  h->maxcharge = maxcharge;
-  h->charge_arg = charge;
-  h->maxiter = maxiter;
+  set_inputs(ps, h, charge, eps, maxcharge, maxiter);
   int st;
   if ((st = check_cuda(cudaMemcpyAsync(ps->dctrl, h, offsetof(SolveCtrl, charge),
                                        cudaMemcpyHostToDevice, s),
@@ -442,8 +542,15 @@ static int stage_out(gfd_poisson* ps, double* phi, cudaStream_t s) {
   const int64_t n0 = ps->L[0].n;
   double* phi_int = ps->precision == GFD_POISSON_FP64 ? static_cast<double*>(ps->L[0].phi[0])
                                                       : ps->phi64;
-  int st = check_cuda(cudaMemcpyAsync(phi, phi_int, n0 * 8, cudaMemcpyDeviceToDevice, s),
-                      "cudaMemcpyAsync(phi)");
+  int st;
+  if (ps->rho_gauss) {
+    // The charged non-periodic branch adds the Gaussian's potential back.
+    launch_k(finish_kernel, grid_for(n0), 256, 0, s, phi, phi_int, ps->dctrl, (long long)n0);
+    st = check_launch("finish_kernel");
+  } else {
+    st = check_cuda(cudaMemcpyAsync(phi, phi_int, n0 * 8, cudaMemcpyDeviceToDevice, s),
+                    "cudaMemcpyAsync(phi)");
+  }
   if (st) return st;
   return check_cuda(cudaMemcpyAsync(ps->hctrl, ps->dctrl, sizeof(SolveCtrl),
                                     cudaMemcpyDeviceToHost, s),
@@ -576,10 +683,9 @@ extern "C" int gfd_poisson_create(int levels, gfd_operator* const* ops,
   ps->npartials = std::max<int64_t>(op_partials(ops[0], GFD_FLOAT64, OP_RESIDUAL, 1), kRedBlocks);
   const size_t o_part = take(sizeof(double) * ps->npartials);
   const size_t o_ctrl = take(sizeof(SolveCtrl));
-  if (cudaMalloc(&ps->pool, off) != cudaSuccess) {
-    cudaGetLastError();
+  if (int st = dev_malloc(&ps->pool, off, "cudaMalloc of the level hierarchy")) {
     delete ps;
-    return set_error(GFD_ENOMEM, "cudaMalloc of the level hierarchy failed");
+    return st;
   }
   if (cudaMallocHost(reinterpret_cast<void**>(&ps->hctrl), sizeof(SolveCtrl)) != cudaSuccess) {
     cudaGetLastError();
@@ -604,6 +710,11 @@ extern "C" int gfd_poisson_create(int levels, gfd_operator* const* ops,
   }
   ps->partials = reinterpret_cast<double*>(base + o_part);
   ps->dctrl = reinterpret_cast<SolveCtrl*>(base + o_ctrl);
+  const int* per = ops[0]->per;
+  ps->bc_kind = per[0] && per[1] && per[2] ? kBcPeriodic
+                : !per[0] && !per[1] && !per[2] ? kBcNone
+                                                 : kBcMixed;
+  ps->madelung = std::nan("");
   *out = ps;
   return GFD_OK;
 }
@@ -614,7 +725,110 @@ extern "C" int gfd_poisson_destroy(gfd_poisson* ps) {
   if (ps->graph) cudaGraphDestroy(ps->graph);
   if (ps->pool) cudaFree(ps->pool);
   if (ps->hctrl) cudaFreeHost(ps->hctrl);
+  if (ps->rho_gauss) cudaFree(ps->rho_gauss);
   delete ps;
+  return GFD_OK;
+}
+
+extern "C" int gfd_poisson_load_gauss(gfd_poisson* ps, const double h_cv[9],
+                                      const int64_t beg_c[3], const double center_v[3], double a,
+                                      void* stream) {
+  if (!ps || !h_cv || !beg_c || !center_v) return set_error(GFD_EINVAL, "null argument");
+  if (!(a > 0.0)) return set_error(GFD_EINVAL, "the Gaussian's exponent must be positive");
+  const gfd_operator* op = ps->L[0].op;
+  const int64_t n0 = ps->L[0].n;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st;
+  if (!ps->rho_gauss) {
+    // One allocation for the Gaussian and its potential (phi_gauss follows).
+    void* p = nullptr;
+    if ((st = dev_malloc(&p, 2 * n0 * sizeof(double), "cudaMalloc(compensating Gaussian)")))
+      return st;
+    ps->rho_gauss = static_cast<double*>(p);
+    ps->phi_gauss = ps->rho_gauss + n0;
+  }
+  GaussGeom geo;
+  for (int i = 0; i < 9; i++) geo.h[i] = h_cv[i];
+  for (int i = 0; i < 3; i++) {
+    geo.center[i] = center_v[i];
+    geo.beg[i] = (int)beg_c[i];
+    geo.n[i] = op->n[i];
+  }
+  geo.a = a;
+  launch_k(gauss_kernel, grid_for(n0), 256, 0, s, ps->rho_gauss, ps->phi_gauss, geo,
+           (long long)n0);
+  if ((st = check_launch("gauss_kernel"))) return st;
+  return check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize(gauss)");
+}
+
+extern "C" int gfd_poisson_set_madelung(gfd_poisson* ps, double madelung) {
+  if (!ps) return set_error(GFD_EINVAL, "null solver");
+  if (!std::isfinite(madelung)) return set_error(GFD_EINVAL, "Madelung shift must be finite");
+  ps->madelung = madelung;
+  return GFD_OK;
+}
+
+// madelung(cell_cv) of gpaw/utilities/ewald.py:148 with the Ewald class of
+// ewald.py:12-146 evaluated at r = r_B = 0 for one probe charge q = -1 that
+// is excluded from the central cell: real-space images erfc(G|l|)/|l| (l != 0,
+// 3 shells either side), reciprocal sum pi/(V G^2) sum_g exp(-x)/x
+// (x = g^2/(4 G^2), g != 0, 9 shells), minus the excluded charge's
+// 2 G / sqrt(pi), plus the homogeneous background pi / (G^2 V);
+// G = 5 / the longest lattice vector.
+extern "C" int gfd_madelung(const double cell_cv[9], double* out) {
+  if (!cell_cv || !out) return set_error(GFD_EINVAL, "null argument");
+  const double* a1 = cell_cv;
+  const double* a2 = cell_cv + 3;
+  const double* a3 = cell_cv + 6;
+  const double det = a1[0] * (a2[1] * a3[2] - a2[2] * a3[1]) -
+                     a1[1] * (a2[0] * a3[2] - a2[2] * a3[0]) +
+                     a1[2] * (a2[0] * a3[1] - a2[1] * a3[0]);
+  const double vol = std::fabs(det);
+  if (!(vol > 0.0)) return set_error(GFD_EINVAL, "singular cell");
+  // Reciprocal vectors b_i = inv(cell).T rows: b1 = (a2 x a3) / det, ...
+  auto cross = [](const double* u, const double* v, double* w) {
+    w[0] = u[1] * v[2] - u[2] * v[1];
+    w[1] = u[2] * v[0] - u[0] * v[2];
+    w[2] = u[0] * v[1] - u[1] * v[0];
+  };
+  double b[3][3];
+  cross(a2, a3, b[0]);
+  cross(a3, a1, b[1]);
+  cross(a1, a2, b[2]);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) b[i][j] /= det;
+  double lmax = 0.0;
+  for (int i = 0; i < 3; i++)
+    lmax = std::max(lmax, cell_cv[3 * i] * cell_cv[3 * i] + cell_cv[3 * i + 1] * cell_cv[3 * i + 1] +
+                              cell_cv[3 * i + 2] * cell_cv[3 * i + 2]);
+  const double G = 5.0 / std::sqrt(lmax);
+  const double pi = 3.141592653589793;
+  const double q = -1.0;
+  double e_r = 0.0;
+  for (int i = -3; i <= 3; i++)
+    for (int j = -3; j <= 3; j++)
+      for (int k = -3; k <= 3; k++) {
+        double l[3];
+        for (int v = 0; v < 3; v++) l[v] = i * a1[v] + j * a2[v] + k * a3[v];
+        const double d = std::sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]);
+        if (d > 1e-5) e_r += std::erfc(G * d) / d;
+      }
+  double e_g = 0.0;
+  for (int i = -9; i <= 9; i++)
+    for (int j = -9; j <= 9; j++)
+      for (int k = -9; k <= 9; k++) {
+        double g[3];
+        for (int v = 0; v < 3; v++) g[v] = 2.0 * pi * (i * b[0][v] + j * b[1][v] + k * b[2][v]);
+        const double g2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+        if (g2 > 1e-10) {
+          const double x = 0.25 * g2 / (G * G);
+          e_g += std::exp(-x) / x;
+        }
+      }
+  double e = q * e_r + q * pi / (vol * G * G) * e_g;
+  e -= q * 2.0 * G / std::sqrt(pi);
+  e += -q * pi / (G * G * vol);
+  *out = e;
   return GFD_OK;
 }
 
@@ -665,9 +879,18 @@ extern "C" int gfd_poisson_autotune(gfd_poisson* ps, int reps, void* stream) {
   return GFD_OK;
 }
 
+static int solve_async_flags(gfd_poisson* ps, double* phi, const double* rho, double charge,
+                             double eps, double maxcharge, int maxiter, void* stream);
+
 extern "C" int gfd_poisson_solve_async(gfd_poisson* ps, double* phi, const double* rho,
                                        double charge, double eps, double maxcharge, int maxiter,
                                        void* stream) {
+  if (ps) ps->zero_init = 0;
+  return solve_async_flags(ps, phi, rho, charge, eps, maxcharge, maxiter, stream);
+}
+
+static int solve_async_flags(gfd_poisson* ps, double* phi, const double* rho, double charge,
+                             double eps, double maxcharge, int maxiter, void* stream) {
   if (!ps) return set_error(GFD_EINVAL, "null solver");
   if (!phi || !rho) return set_error(GFD_EINVAL, "null array pointer");
   if (maxiter < 1) return set_error(GFD_EINVAL, "maxiter must be >= 1");
@@ -682,9 +905,19 @@ extern "C" int gfd_poisson_solve_async(gfd_poisson* ps, double* phi, const doubl
 extern "C" int gfd_poisson_result(const gfd_poisson* ps, int* niter, double* error) {
   if (!ps) return set_error(GFD_EINVAL, "null solver");
   const SolveCtrl* h = ps->hctrl;
-  if (h->status == GFD_EUNSUPPORTED)
+  if (h->status == GFD_ENEEDGAUSS)
+    return set_error(GFD_ENEEDGAUSS,
+                     "charged non-periodic system: load the compensating Gaussian first "
+                     "(gfd_poisson_load_gauss); phi is unchanged");
+  if (h->status == GFD_EUNSUPPORTED) {
+    if (h->skip) return set_error(GFD_EUNSUPPORTED, "unused batch slot");
+    if (ps->bc_kind == kBcPeriodic)
+      return set_error(GFD_EUNSUPPORTED,
+                       "charged periodic system: set the Madelung shift first "
+                       "(gfd_poisson_set_madelung)");
     return set_error(GFD_EUNSUPPORTED,
-                     "charged system: only the charge-neutral branch of solve() is provided");
+                     "charged system with mixed boundary conditions is not supported");
+  }
   if (niter) *niter = h->niter;
   if (error) *error = h->err;
   if (h->niter >= h->maxiter)
@@ -696,7 +929,16 @@ extern "C" int gfd_poisson_result(const gfd_poisson* ps, int* niter, double* err
 extern "C" int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho, double charge,
                                  double eps, double maxcharge, int maxiter, int* niter_out,
                                  double* error_out, void* stream) {
+  return gfd_poisson_solve_ex(ps, phi, rho, charge, eps, maxcharge, maxiter, 0, niter_out,
+                              error_out, stream);
+}
+
+extern "C" int gfd_poisson_solve_ex(gfd_poisson* ps, double* phi, const double* rho,
+                                    double charge, double eps, double maxcharge, int maxiter,
+                                    int flags, int* niter_out, double* error_out, void* stream) {
   if (!ps) return set_error(GFD_EINVAL, "null solver");
+  if (flags & ~GFD_SOLVE_ZERO_INITIAL_PHI) return set_error(GFD_EINVAL, "unknown solve flags");
+  ps->zero_init = (flags & GFD_SOLVE_ZERO_INITIAL_PHI) ? 1 : 0;
   if (!phi || !rho) return set_error(GFD_EINVAL, "null array pointer");
   if (maxiter < 1) return set_error(GFD_EINVAL, "maxiter must be >= 1");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -708,8 +950,7 @@ extern "C" int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho
   }();
   int st;
   if (!eager) {
-    if ((st = gfd_poisson_solve_async(ps, phi, rho, charge, eps, maxcharge, maxiter, stream)))
-      return st;
+    if ((st = solve_async_flags(ps, phi, rho, charge, eps, maxcharge, maxiter, stream))) return st;
   } else {
     if ((st = stage_in(ps, phi, rho, charge, eps, maxcharge, maxiter, s))) return st;
     if ((st = solve_eager(ps, s))) return st;
@@ -818,20 +1059,20 @@ extern "C" int gfd_poisson_batch_solve_async(gfd_poisson_batch* b, double* const
       return set_error(GFD_EINVAL, "phi and rho of a batch slot must both be given or both null");
   for (int i = 0; i < n; i++) {
     if (!phis[i]) {
-      // Unused slot: an infinite charge marks the solve as refused, so it
-      // runs no V-cycle; its arrays are neither read nor written.
+      // Unused slot: marked skipped, so it runs no V-cycle; its arrays are
+      // neither read nor written.
       gfd_poisson* ps = b->solvers[i];
       SolveCtrl* h = ps->hctrl;
-      h->eps = eps;
-      h->maxcharge = maxcharge;
-      h->charge_arg = INFINITY;
-      h->maxiter = maxiter;
+      ps->zero_init = 0;
+      set_inputs(ps, h, std::nan(""), eps, maxcharge, maxiter);
+      h->skip = 1;
       if ((st = check_cuda(cudaMemcpyAsync(ps->dctrl, h, offsetof(SolveCtrl, charge),
                                            cudaMemcpyHostToDevice, s),
                            "cudaMemcpyAsync(controls)")))
         return st;
       continue;
     }
+    b->solvers[i]->zero_init = 0;
     if ((st = stage_in(b->solvers[i], phis[i], rhos[i], std::nan(""), eps, maxcharge, maxiter, s)))
       return st;
   }

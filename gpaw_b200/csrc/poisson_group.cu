@@ -687,10 +687,9 @@ int group_create(gfd_poisson* const* solvers, int n, PoissonGroup** out) {
   const size_t o_tile0 = take(sizeof(int) * n);
   const size_t o_ntile = take(sizeof(int) * n);
   const size_t o_dv = take(sizeof(double) * n);
-  if (cudaMalloc(&G->mem, off) != cudaSuccess) {
-    cudaGetLastError();
+  if (int st = dev_malloc(&G->mem, off, "cudaMalloc of the batch tables")) {
     delete G;
-    return set_error(GFD_ENOMEM, "cudaMalloc of the batch tables failed");
+    return st;
   }
   unsigned char* base = static_cast<unsigned char*>(G->mem);
   G->d_items = base + o_items;

@@ -21,20 +21,29 @@ struct Level {
 };
 
 // Solve controls shared by host and device.  The host writes the inputs
-// before each launch and reads the outputs after it.
+// (up to `charge`) before each launch and reads the outputs after it.
 struct SolveCtrl {
   double eps;
   double maxcharge;
   double charge_arg;  // NaN: use the integral of rho
   int maxiter;
-  int pad0;
+  int zero_init;      // charged branches start from phi = 0 (zero_initial_phi)
+  const double* rho_gauss;  // L = 0 Gaussian of the non-periodic charged branch (or null)
+  const double* phi_gauss;  // its potential
+  double madelung;    // periodic charged branch: potential shift per unit charge (NaN: unset)
+  int bc_kind;        // kBcPeriodic, kBcNone or kBcMixed (level-0 boundary conditions)
+  int skip;           // an unused batch slot: no solve
   double charge;      // integral of rho times dv
   double bg;          // background charge density removed from rho
+  double gq;          // non-periodic charged branch: the Gaussian's weight (charge / sqrt(4 pi))
+  double shift;       // periodic charged branch: charge * madelung, added to phi
   double err;         // last residual norm sum(r^2) dv
   double sum;         // scratch scalar (sum of phi)
   int niter;
-  int status;         // GFD_OK or GFD_EUNSUPPORTED (charged)
+  int status;         // GFD_OK, GFD_EUNSUPPORTED (refused), GFD_ENEEDGAUSS
 };
+
+enum { kBcMixed = 0, kBcPeriodic = 1, kBcNone = 2 };
 
 struct gfd_poisson {
   int levels = 0;
@@ -59,6 +68,14 @@ struct gfd_poisson {
   cudaGraphExec_t exec = nullptr;
   int device = -1;
   gfd_operator* B = nullptr;  // Mehrstellen right-hand side (not owned)
+  int bc_kind = kBcMixed;
+  // Charged branches (gpaw/poisson.py:139-191): the L = 0 Gaussian and its
+  // potential on the level-0 grid (owned, allocated by gfd_poisson_load_gauss)
+  // and the Madelung shift per unit charge (NaN until set).
+  double* rho_gauss = nullptr;
+  double* phi_gauss = nullptr;
+  double madelung = 0.0;
+  int zero_init = 0;
 };
 
 namespace gfd {

@@ -101,11 +101,11 @@ extern "C" int gfd_preconditioner_create(gfd_operator* kin0, gfd_operator* kin1,
   const size_t esz = dtype_size(dtype);
   const int64_t lv[7] = {pc->n[1], pc->n[1], pc->n[1], pc->n[2], pc->n[2], pc->n[2], pc->n[0]};
   for (int i = 0; i < 7; i++) {
-    if (cudaMalloc(&pc->buf[i], size_t(lv[i]) * size_t(block) * esz) != cudaSuccess) {
-      cudaGetLastError();
+    if (int st = dev_malloc(&pc->buf[i], size_t(lv[i]) * size_t(block) * esz,
+                            "cudaMalloc of preconditioner scratch")) {
       release(pc);
       delete pc;
-      return set_error(GFD_ENOMEM, "cudaMalloc of preconditioner scratch failed");
+      return st;
     }
   }
   *out = pc;

@@ -53,7 +53,11 @@ struct StarParams {
 
 // Asynchronous global->shared copies (sm_80+ cp.async).  A source size of 0
 // writes zeros (zero boundary points); the source address is then unused but
-// kept valid.
+// kept valid.  16-byte copies use the L1-allocating form (.ca): measured on
+// B200, the cache-bypass form (.cg) fetched one 32-byte L2 sector per lane
+// and wrote shared memory one lane at a time (about 28 shared-store
+// wavefronts per warp copy of 512 contiguous bytes, against 4.5 for .ca), so
+// it moved twice the bytes from L2.
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
@@ -62,7 +66,7 @@ __device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid)
   const unsigned d = smem_addr(dst);
   const int n = valid ? BYTES : 0;
   if constexpr (BYTES == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n)
                  : "memory");
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
@@ -213,7 +217,7 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
       const int st = (P - pbeg) % S;
       const unsigned sbase = smem0 + unsigned(st * CELLS * sizeof(V));
       int xside;
-      const int xs = wrap_axis(P, p.n0, p.per0, xside);
+      const int xs = wrap_plane(P, p.n0, p.per0, xside);
       const char* src = inb_c + size_t(xs >= 0 ? xs : 0) * plane_b;
       const unsigned zmask = xs >= 0 ? czero : ~0u;
 #pragma unroll
@@ -221,7 +225,7 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
         if (!(clive >> i & 1u)) continue;
         const unsigned n = (zmask >> i & 1u) ? 0u : unsigned(sizeof(V));
         if constexpr (sizeof(V) == 16)
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sbase + cdst[i]),
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sbase + cdst[i]),
                        "l"(src + csrc[i]), "r"(n)
                        : "memory");
         else
@@ -239,7 +243,7 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
             const unsigned n = own_in[j] ? unsigned(sizeof(V)) : 0u;
             const unsigned d = rbase + unsigned(j * BZ * sizeof(V));
             if constexpr (sizeof(V) == 16)
-              asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d),
+              asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d),
                            "l"(rsrc + own_b[j]), "r"(n)
                            : "memory");
             else
@@ -334,7 +338,7 @@ star_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restrict__
         }
 
         int xside;
-        const int xs = wrap_axis(pl, p.n0, p.per0, xside);
+        const int xs = wrap_plane(pl, p.n0, p.per0, xside);
         if (xs >= 0) {
           if constexpr (vt<V>::NC == 2) {
             if (xside >= 0) {
@@ -520,7 +524,7 @@ general_kernel(const V* __restrict__ in, V* __restrict__ out, const V* __restric
   for (int pl = x0 - mp; pl < x1 + mp; ++pl) {
     V* slot = ring + ((pl - (x0 - mp)) % NR) * CELLS;
     int xside;
-    int xs = wrap_axis(pl, p.n0, p.per0, xside);
+    int xs = wrap_plane(pl, p.n0, p.per0, xside);
     for (int c = t; c < CELLS; c += NT) {
       int sy = c / SZ, sz = c % SZ;
       int ysd, zsd;

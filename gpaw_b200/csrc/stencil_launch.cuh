@@ -8,7 +8,9 @@
 
 #include "internal.h"
 #include "stencil.cuh"
+#include "stencil_split.cuh"
 #include "stencil_tma.cuh"
+#include "stencil_tmasplit.cuh"
 
 namespace gfd {
 
@@ -31,6 +33,7 @@ inline TileDims tile_dims(int tile) {
     case TILE_NARROW: return {8, 8, 64};
     case TILE_MID: return {16, 16, 128};
     case TILE_SHORT: return {32, 8, 128};
+    case TILE_SPLIT: return {32, 4 * GFD_SPLIT_VY, 128};
     default: return {32, 16, 128};
   }
 }
@@ -117,12 +120,17 @@ int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t n
 // radii up to 3 only, which keeps the number of kernels in check.
 constexpr int kMaxComplexRelaxR = 3;
 
-// The short tile exists for complex128 apply up to radius 4 (beyond, its
-// 2R + 1 partial sums per row do not fit 128 registers).
+// The short tile exists for complex128 apply (and apply with a potential)
+// up to radius 4 (beyond, its 2R + 1 partial sums per row do not fit 128
+// registers).  It is the built-in choice for those launches: four CTAs of
+// 128 threads per SM measured fastest on B200 (the 512-band 96^3 Laplace:
+// 3730 GB/s against 3120 for the 32 x 16 tile, 3100 for the lane-pair
+// kernel and 3270 for its TMA-staged form, one box, 16-byte cp.async in the
+// L1-allocating form).
 constexpr int kMaxShortR = 4;
 template <class V, int R, int MODE>
 constexpr bool has_short_tile() {
-  return sizeof(V) >= 16 && MODE == MODE_APPLY && R <= kMaxShortR;
+  return sizeof(V) >= 16 && (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) && R <= kMaxShortR;
 }
 
 template <class V, int R, int MODE>
@@ -168,6 +176,99 @@ int star_dispatch(const gfd_operator* op, int tile, const V* in, V* out, const V
 #undef GFD_STAR_SMALL
 #undef GFD_STAR_WIDE
   return set_error(GFD_EUNSUPPORTED, "star stencil radius out of range");
+}
+
+// ---------------------------------------------------------------------------
+// Complex bands with the real and imaginary parts on lane pairs
+// (stencil_split.cuh): 32 x 16 tile, 4 rows x 2 columns per lane, four
+// pipeline stages (three with a staged source term), three CTAs per SM.
+// ---------------------------------------------------------------------------
+constexpr int kSplitVY = GFD_SPLIT_VY, kSplitWY = 4;
+
+// GFD_SPLIT=0 in the environment keeps complex bands on star_kernel (for
+// comparisons); the lane-pair kernel is the default.
+
+template <class V>
+inline bool split_eligible(const gfd_operator* op) {
+  return vt<V>::NC == 2 && op->R >= 1 && op->R <= kSplitMaxR && split_enabled();
+}
+
+template <class V, int R, int MODE>
+int split_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
+             const StarParams<typename vt<V>::S>& p, const LaunchGeom& g, cudaStream_t s) {
+  constexpr bool RHO = MODE == MODE_JACOBI || MODE == MODE_RESIDUAL;
+  constexpr int S = RHO ? 3 : 4;
+  constexpr size_t smem = split_smem_bytes<V, R, kSplitVY, kSplitWY, S, MODE>();
+  auto kern = star_split_kernel<V, R, kSplitVY, kSplitWY, S, MODE>;
+  int st = raise_smem_limit(kern, smem, "cudaFuncSetAttribute(star_split_kernel)");
+  if (st) return st;
+  if ((st = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            int(cudaSharedmemCarveoutMaxShared)),
+                       "cudaFuncSetAttribute(carveout)")))
+    return st;
+  const long long band = (long long)op->n[0] * op->n[1] * op->n[2];
+  for (int64_t b0 = 0; b0 < nin; b0 += g.bands_per_launch) {
+    int64_t nb = std::min<int64_t>(g.bands_per_launch, nin - b0);
+    dim3 grid(g.grid.x, g.grid.y, (unsigned)(nb * g.nxc));
+    launch_k(kern, grid, 32 * kSplitWY, smem, s, in + b0 * band, out + b0 * band,
+             rho ? rho + b0 * band : nullptr, p);
+  }
+  return check_launch("star_split_kernel");
+}
+
+template <class V, int MODE>
+int split_dispatch(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
+                   const StarParams<typename vt<V>::S>& p, const LaunchGeom& g, cudaStream_t s) {
+  if constexpr (vt<V>::NC == 2) {
+    switch (op->R) {
+      case 1: return split_go<V, 1, MODE>(op, in, out, rho, nin, p, g, s);
+      case 2: return split_go<V, 2, MODE>(op, in, out, rho, nin, p, g, s);
+      case 3: return split_go<V, 3, MODE>(op, in, out, rho, nin, p, g, s);
+    }
+  }
+  return set_error(GFD_EUNSUPPORTED, "lane-pair stencil: complex bands, radius <= 3");
+}
+
+// ---------------------------------------------------------------------------
+// complex128 bands on full-row tiles staged by TMA, real and imaginary parts
+// on lane pairs (stencil_tmasplit.cuh).  Takes grids up to 128 columns
+// (32 ng, ng <= kTsMaxNG) whose rows tile evenly along a periodic axis 1, and
+// a potential only on an even number of columns (its rows must start on a
+// 16-byte boundary).
+// ---------------------------------------------------------------------------
+}  // namespace gfd
+GFD_DECLARE_TS_ENTRY(1)
+GFD_DECLARE_TS_ENTRY(2)
+GFD_DECLARE_TS_ENTRY(3)
+GFD_DECLARE_TS_ENTRY(4)
+namespace gfd {
+
+inline int ts_ng(const gfd_operator* op) { return (op->n[2] + 31) / 32; }
+
+template <class V>
+inline bool ts_eligible(const gfd_operator* op, int mode, const void* in, const void* rho) {
+  if constexpr (!std::is_same_v<V, cplx<double>>) {
+    return false;
+  } else {
+    if (!tmasplit_enabled() || op->R < 1 || op->R > kSplitMaxR) return false;
+    if (ts_ng(op) > kTsMaxNG) return false;
+    if (op->per[1] && op->n[1] % kTsBY) return false;
+    if (mode == OP_POTENTIAL && (op->n[2] & 1)) return false;
+    auto aligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    return aligned(in) && (!rho || aligned(rho));
+  }
+}
+
+inline int ts_dispatch(const gfd_operator* op, int kmode, const cplx<double>* in,
+                       cplx<double>* out, const cplx<double>* rho, const void* pot, int64_t nin,
+                       const StarParams<double>& p, int cps, cudaStream_t s) {
+  switch (ts_ng(op)) {
+    case 1: return ts_launch_1(op, kmode, in, out, rho, pot, nin, p, cps, s);
+    case 2: return ts_launch_2(op, kmode, in, out, rho, pot, nin, p, cps, s);
+    case 3: return ts_launch_3(op, kmode, in, out, rho, pot, nin, p, cps, s);
+    case 4: return ts_launch_4(op, kmode, in, out, rho, pot, nin, p, cps, s);
+  }
+  return set_error(GFD_EUNSUPPORTED, "TMA lane-pair stencil: at most 128 columns");
 }
 
 // ---------------------------------------------------------------------------
@@ -321,18 +422,50 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
     }
   }
   // Radii above 2 have the wide tile only (and the short one for complex128
-  // apply): any other plan tile falls back to the built-in choice, so the
-  // geometry always matches the kernel launched.
+  // apply); complex bands up to radius 3 have the lane-pair tile, their
+  // built-in choice wherever the wide tile would be picked.  Any other plan
+  // tile falls back to the built-in choice, so the geometry always matches
+  // the kernel launched.
   int tile = pick_tile(op);
+  const bool split = split_eligible<V>(op);
+  const bool tsplit = ts_eligible<V>(op, mode, in, rho);
+  const bool shortok =
+      sizeof(V) >= 16 && (mode == OP_APPLY || mode == OP_POTENTIAL) && op->R <= kMaxShortR;
+  if (shortok && tile == TILE_WIDE) tile = TILE_SHORT;
   if (tuned) {
     if (plan.tile == TILE_SHORT)
-      tile = sizeof(V) >= 16 && mode == OP_APPLY && op->R <= kMaxShortR ? TILE_SHORT : tile;
-    else if (op->R <= 2)
+      tile = shortok ? TILE_SHORT : tile;
+    else if (plan.tile == TILE_TMASPLIT)
+      tile = tsplit ? TILE_TMASPLIT : tile;
+    else if (plan.tile == TILE_SPLIT)
+      tile = split ? TILE_SPLIT : tile;
+    else if (op->R <= 2 || plan.tile == TILE_WIDE)
       tile = plan.tile;
+  }
+  if constexpr (std::is_same_v<V, cplx<double>>) {
+    if (tile == TILE_TMASPLIT) {
+      const int cps = tuned ? plan.cps : 0;
+      if (mode == OP_POTENTIAL)
+        return ts_dispatch(op, MODE_POTENTIAL, vin, vout, nullptr, rho, nin, p, cps, s);
+      if (mode == OP_JACOBI || mode == OP_JACOBI_NEG)
+        return ts_dispatch(op, MODE_JACOBI, vin, vout, vrho, nullptr, nin, p, cps, s);
+      if (mode == OP_RESIDUAL)
+        return ts_dispatch(op, MODE_RESIDUAL, vin, vout, vrho, nullptr, nin, p, cps, s);
+      return ts_dispatch(op, MODE_APPLY, vin, vout, nullptr, nullptr, nin, p, cps, s);
+    }
   }
   LaunchGeom g = star_geom(op, tile, nin, op->R, tuned ? plan.cps : 0);
   p.nxc = g.nxc;
   p.x_chunk = g.x_chunk;
+  if (tile == TILE_SPLIT) {
+    if (mode == OP_POTENTIAL)
+      return split_dispatch<V, MODE_POTENTIAL>(op, vin, vout, nullptr, nin, p, g, s);
+    if (mode == OP_JACOBI || mode == OP_JACOBI_NEG)
+      return split_dispatch<V, MODE_JACOBI>(op, vin, vout, vrho, nin, p, g, s);
+    if (mode == OP_RESIDUAL)
+      return split_dispatch<V, MODE_RESIDUAL>(op, vin, vout, vrho, nin, p, g, s);
+    return split_dispatch<V, MODE_APPLY>(op, vin, vout, nullptr, nin, p, g, s);
+  }
   if (mode == OP_POTENTIAL)
     return star_dispatch<V, MODE_POTENTIAL>(op, tile, vin, vout, nullptr, nin, p, g, nullptr, s);
   if (mode == OP_JACOBI || mode == OP_JACOBI_NEG)

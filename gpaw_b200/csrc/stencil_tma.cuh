@@ -263,7 +263,7 @@ star_tma_kernel(cplx<double>* __restrict__ out, const StarParams<double> p,
         const V* st = stages + s * St::CELLS;
         const int pl = pbeg + i;
         int xside;
-        const int xs = wrap_axis(pl, p.n0, p.per0, xside);
+        const int xs = wrap_plane(pl, p.n0, p.per0, xside);
         V own[VY];
         if (!failed) {
           if (pl >= x0 && pl < x1) {

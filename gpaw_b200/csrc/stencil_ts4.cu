@@ -1,0 +1,5 @@
+// stencil_ts4.cu -- star_tmasplit_kernel instantiations for 4 column group(s)
+// of 32 (one translation unit per count, so they compile in parallel).
+#include "stencil_tmasplit.cuh"
+
+GFD_DEFINE_TS_ENTRY(4)

@@ -303,3 +303,20 @@ def Laplace(gd, scale=1.0, n=1, dtype=float, allocate=True):
     if n == 9:
         raise NotImplementedError('FTLaplace (n=9) is an FFT operator, not provided')
     return NewGUCLaplace(gd, scale, n, dtype, allocate)
+
+
+def apply_pseudo_hamiltonian(kin, psit_xG, Htpsit_xG, vt_G, phase_cd=None):
+    """Htpsit_xG = kin psit_xG + vt_G psit_xG over a band batch: GPAW's
+    FDWaveFunctions.apply_pseudo_hamiltonian (gpaw/wavefunctions/fd.py:50-52),
+    the kinetic apply followed by Hamiltonian.apply_local_potential
+    (gpaw/hamiltonian.py:371-398, Htpsit += psit * vt), as one kernel pass:
+    the potential joins the stencil's centre weight, so each band is read
+    once and written once (FDOperator.apply_with_potential).
+
+    kin: the kinetic FDOperator (Laplace(gd, -0.5, nn, dtype)); vt_G: the spin
+    channel's local potential on the same grid (float64 for float64/complex128
+    bands, float32 for float32/complex64); phase_cd: the k-point's Bloch phases
+    for complex bands."""
+    if not isinstance(kin, FDOperator):
+        raise TypeError('kin must be an FDOperator')
+    kin.apply_with_potential(psit_xG, Htpsit_xG, vt_G, phase_cd)

@@ -26,8 +26,18 @@ import numpy as np
 from . import _lib
 from .errors import PoissonConvergenceError  # noqa: F401  (re-exported)
 from .fd_operators import Laplace, LaplaceA, LaplaceB
-from .tensors import require_device, stream_of
+from .tensors import require_device, stream_of, stream_of_device
 from .transformers import Transformer
+
+
+def madelung(cell_cv):
+    """Potential shift per unit charge of a charged periodic system:
+    madelung(cell_cv) of gpaw/utilities/ewald.py:148 (Ewald sum, computed by
+    libgpawfd on the host)."""
+    c, cp = _lib.f64(np.asarray(cell_cv, float).reshape(3, 3))
+    out = _lib.ctypes.c_double(0.0)
+    _lib.check(_lib.lib.gfd_madelung(cp, _lib.ctypes.byref(out)), 'madelung')
+    return out.value
 
 
 class PoissonSolver:
@@ -112,6 +122,36 @@ class PoissonSolver:
         if self.B is not None:
             _lib.check(_lib.lib.gfd_poisson_set_rhs_operator(handle, self.B.operator),
                        'PoissonSolver')
+        if self.gd.pbc_c.all():
+            # charged periodic systems: the Madelung shift per unit charge
+            # (charged_periodic_correction, gpaw/poisson.py:143-151)
+            if self.charged_periodic_correction is None:
+                self.charged_periodic_correction = madelung(self.gd.cell_cv)
+            _lib.check(_lib.lib.gfd_poisson_set_madelung(handle,
+                                                         self.charged_periodic_correction),
+                       'PoissonSolver')
+        if load_gauss:
+            self.load_gauss()
+
+    def load_gauss(self):
+        """The compensating L = 0 Gaussian of charged non-periodic systems
+        and its potential, on the device (gpaw/poisson.py:118-123;
+        Gaussian(gd) of gpaw/utilities/gauss.py:47-82: exponent
+        4 * 19 * max_c sum_v icell_cv^2, centred in the cell)."""
+        if self.solver is None:
+            self.initialize()
+        if getattr(self, '_gauss_loaded', False):
+            return
+        gd = self.gd
+        a = 4 * 19.0 * (gd.icell_cv ** 2).sum(1).max()
+        center = 0.5 * gd.cell_cv.sum(0)
+        h, hp = _lib.f64(gd.h_cv)
+        b, bp = _lib.i64(gd.beg_c)
+        c, cp = _lib.f64(center)
+        _lib.check(_lib.lib.gfd_poisson_load_gauss(self.solver, hp, bp, cp, float(a),
+                                                   stream_of_device(gd.device)),
+                   'PoissonSolver.load_gauss')
+        self._gauss_loaded = True
 
     def __del__(self):
         h = getattr(self, 'solver', None)
@@ -121,22 +161,33 @@ class PoissonSolver:
             self.solver = None
 
     def solve(self, phi, rho, charge=None, eps=None, maxcharge=1e-6, zero_initial_phi=False):
-        """Solve nabla^2 phi = -4 pi rho for a charge-neutral rho; phi holds
-        the initial guess and receives the solution.  Returns the number of
-        V-cycles.  Raises PoissonConvergenceError after maxiter V-cycles."""
+        """Solve nabla^2 phi = -4 pi rho; phi holds the initial guess and
+        receives the solution.  Returns the number of V-cycles.  The
+        reference's three branches (gpaw/poisson.py:124-191): neutral, charged
+        periodic (Madelung shift), charged non-periodic (compensating
+        Gaussian, loaded on first need); charged with mixed boundary
+        conditions raises NotImplementedError.  zero_initial_phi starts the
+        charged branches from phi = 0, as the reference (the neutral branch
+        keeps phi).  Raises PoissonConvergenceError after maxiter V-cycles."""
         if self.solver is None:
             self.initialize()
         self._check_arrays(phi, rho)
         if eps is None:
             eps = self.eps
-        if zero_initial_phi:
-            phi.zero_()
+        flags = _lib.GFD_SOLVE_ZERO_INITIAL_PHI if zero_initial_phi else 0
         niter = _lib.ctypes.c_int(0)
         err = _lib.ctypes.c_double(0.0)
-        status = _lib.lib.gfd_poisson_solve(
-            self.solver, phi.data_ptr(), rho.data_ptr(),
-            _lib.nan() if charge is None else float(charge), float(eps), float(maxcharge),
-            int(self.maxiter), _lib.ctypes.byref(niter), _lib.ctypes.byref(err), stream_of(phi))
+        for attempt in range(2):
+            status = _lib.lib.gfd_poisson_solve_ex(
+                self.solver, phi.data_ptr(), rho.data_ptr(),
+                _lib.nan() if charge is None else float(charge), float(eps), float(maxcharge),
+                int(self.maxiter), flags, _lib.ctypes.byref(niter), _lib.ctypes.byref(err),
+                stream_of(phi))
+            if status != _lib.GFD_ENEEDGAUSS or attempt:
+                break
+            # A charged non-periodic rho: phi is unchanged; load the Gaussian
+            # (gpaw/poisson.py:162-164) and solve again.
+            self.load_gauss()
         self.niter = niter.value
         self.error = err.value
         _lib.check(status, 'PoissonSolver.solve')

@@ -22,6 +22,18 @@ PoissonServer(...)
     Completions are found by polling the oldest launch of each stream, and
     each pod returns to its pool.  Latency is completion minus arrival.
     Solves never share buffers, so a result is the same alone and in the mix.
+    Each pod owns its requests' potential buffers, so the serving loop makes
+    no device allocation once the pods exist (an allocation would stall the
+    launches in flight).
+
+    Failures are per request, on the host: a request whose `deadline`
+    (seconds after its arrival) passes while it waits is dropped
+    ('expired'); one whose `cancel_at` (seconds from the start of the run)
+    passes is dropped if it waits and its result discarded if it is in
+    flight ('cancelled'; a launch on the GPU is never interrupted); a pod
+    that cannot be created (over the memory budget, or the device allocation
+    fails) leaves the request waiting while other launches are in flight and
+    rejects it when nothing is ('rejected').
 """
 import collections
 import time
@@ -107,14 +119,19 @@ def grid_for(N, h_bohr, pbc=False, device=None):
 
 
 class Request:
+    """One solve: grid size N, arrival time (seconds from the start of the
+    run), rho on the device; optional deadline (seconds after arrival by
+    which it must be admitted) and cancel_at (seconds from the start)."""
     __slots__ = ('rid', 'N', 'arrival', 'rho', 'admit', 'done', 'niter', 'error', 'phi',
-                 'status')
+                 'status', 'deadline', 'cancel_at')
 
-    def __init__(self, rid, N, arrival, rho):
+    def __init__(self, rid, N, arrival, rho, deadline=None, cancel_at=None):
         self.rid = rid
         self.N = N
         self.arrival = arrival
         self.rho = rho
+        self.deadline = deadline
+        self.cancel_at = cancel_at
         self.admit = None
         self.done = None
         self.niter = None
@@ -125,14 +142,16 @@ class Request:
 
 class _Pod:
     """`slots` solvers of one grid size that launch together: one graph
-    launch (a PoissonBatch) serves up to `slots` requests."""
-    __slots__ = ('N', 'solvers', 'batch', 'nbytes')
+    launch (a PoissonBatch) serves up to `slots` requests; `phis` are the
+    slots' potential buffers."""
+    __slots__ = ('N', 'solvers', 'batch', 'nbytes', 'phis')
 
-    def __init__(self, N, solvers, batch, nbytes):
+    def __init__(self, N, solvers, batch, nbytes, phis):
         self.N = N
         self.solvers = solvers
         self.batch = batch
         self.nbytes = nbytes
+        self.phis = phis
 
 
 class PoissonServer:
@@ -158,33 +177,43 @@ class PoissonServer:
         self.used_bytes = 0
         self.keep_results = keep_results
         self.rejected = 0
+        self.alloc_failures = 0
 
     # -- pod pool --------------------------------------------------------------
     def _new_pod(self, N, slots):
+        """A pod of `slots` solvers of size N, or None when it would exceed
+        the memory budget or its device allocations fail."""
         solvers, need = [], 0
         for _ in range(slots):
             ps = PoissonSolver(self.nn, self.relax, self.eps, precision=self.precision)
             ps.set_grid_descriptor(grid_for(N, self.h, device=self.device))
-            need += ps.nbytes() + 2 * int(np.prod(ps.gd.n_c)) * 8  # + the request's phi
+            need += ps.nbytes() + int(np.prod(ps.gd.n_c)) * 8  # + the slot's phi
             solvers.append(ps)
         if self.used_bytes + need > self.budget:
             return None
-        for ps in solvers:
-            ps.initialize()
-        # Many pods are in flight at once: plain graph branches overlap
-        # better there than grouped launches (measured on B200: 32^3
-        # requests 2.7K/s against 1.2K/s grouped).
-        batch = PoissonBatch(solvers, group=False) if slots > 1 else None
+        try:
+            for ps in solvers:
+                ps.initialize()
+            # Many pods are in flight at once: plain graph branches overlap
+            # better there than grouped launches (measured on B200: 32^3
+            # requests 2.7K/s against 1.2K/s grouped).
+            batch = PoissonBatch(solvers, group=False) if slots > 1 else None
+            shape = tuple(int(x) for x in solvers[0].gd.n_c)
+            phis = [torch.empty(shape, dtype=torch.float64, device=self.device)
+                    for _ in range(slots)]
+        except MemoryError:
+            self.alloc_failures += 1
+            return None  # the solvers release what they hold when collected
         self.used_bytes += need
-        return _Pod(N, solvers, batch, need)
+        return _Pod(N, solvers, batch, need, phis)
 
     def _launch(self, pod, reqs, stream):
-        """Enqueue the requests on the pod's first slots; returns their phis."""
-        phis = []
+        """Enqueue the requests on the pod's first slots (from phi = 0);
+        returns their phis (the pod's buffers)."""
+        phis = pod.phis[:len(reqs)]
         with torch.cuda.stream(stream):
-            for r in reqs:
-                phis.append(torch.zeros(tuple(int(x) for x in pod.solvers[0].gd.n_c),
-                                        dtype=torch.float64, device=self.device))
+            for phi in phis:
+                phi.zero_()
             if pod.batch is None:
                 pod.solvers[0].solve_async(phis[0], reqs[0].rho)
             else:
@@ -245,6 +274,11 @@ class PoissonServer:
         ninflight = 0   # launches in flight
         ev_pool = []
         si = 0
+        rejected0 = self.rejected
+        deadlines = any(r.deadline is not None for r in requests)
+        cancels = sorted((r for r in requests if r.cancel_at is not None),
+                         key=lambda r: r.cancel_at)
+        ci = 0
         t0 = time.perf_counter()
         while pending or ninflight or any(queues.values()):
             now = time.perf_counter() - t0
@@ -255,20 +289,45 @@ class PoissonServer:
                     done = time.perf_counter() - t0
                     for slot, (req, phi) in enumerate(zip(reqs, phis)):
                         req.done = done
+                        if req.status == 'cancelled':
+                            continue  # result discarded
                         try:
                             req.niter, req.error = pod.solvers[slot].result()
                             req.status = 'ok'
                         except Exception as e:  # reported per request
                             req.status = repr(e)
                         if self.keep_results:
-                            req.phi = phi
+                            req.phi = phi.clone()
                     ninflight -= 1
                     self.free[pod.N, len(pod.solvers)].append(pod)
                     ev_pool.append(ev)
+            # cancellations due: waiting or not yet arrived requests are
+            # dropped, in-flight ones have their results discarded
+            while ci < len(cancels) and cancels[ci].cancel_at <= now:
+                r = cancels[ci]
+                ci += 1
+                if r.status is None:
+                    r.status = 'cancelled'
+                    q = queues.get(r.N)
+                    if q is not None and r in q:
+                        q.remove(r)
             # arrivals join the queue of their grid size
             while pending and pending[0].arrival <= now:
                 r = pending.popleft()
+                if r.status == 'cancelled':
+                    continue
                 queues.setdefault(r.N, collections.deque()).append(r)
+            # waiting requests whose admission deadline has passed
+            if deadlines:
+                for N, q in queues.items():
+                    if any(r.deadline is not None and now > r.arrival + r.deadline for r in q):
+                        keep = collections.deque()
+                        for r in q:
+                            if r.deadline is not None and now > r.arrival + r.deadline:
+                                r.status = 'expired'
+                            else:
+                                keep.append(r)
+                        queues[N] = keep
             # admit: sizes in order of their oldest waiting request; each
             # launch takes up to `slots` of that size's waiting requests
             for N in sorted((n for n in queues if queues[n]), key=lambda n: queues[n][0].arrival):
@@ -276,9 +335,9 @@ class PoissonServer:
                 while q and ninflight < self.max_inflight:
                     pod = self._acquire(N, len(q), ninflight)
                     if pod is None:
-                        if not ninflight:  # cannot ever fit
+                        if not ninflight:  # cannot fit now, nor after a retirement
                             req = q.popleft()
-                            req.status = 'rejected: over memory budget'
+                            req.status = 'rejected: no device memory for a solver of this size'
                             self.rejected += 1
                             continue
                         break
@@ -301,11 +360,16 @@ class PoissonServer:
         wall = time.perf_counter() - t0
         done = [r for r in requests if r.status == 'ok']
         lat = np.array([r.done - r.arrival for r in done]) if done else np.zeros(1)
-        return {'requests': len(requests), 'completed': len(done), 'rejected': self.rejected,
+        return {'requests': len(requests), 'completed': len(done),
+                'rejected': self.rejected - rejected0,
+                'expired': sum(r.status == 'expired' for r in requests),
+                'cancelled': sum(r.status == 'cancelled' for r in requests),
+                'failed': sum(r.status not in (None, 'ok', 'expired', 'cancelled') and
+                              not r.status.startswith('rejected') for r in requests),
                 'wall_s': wall, 'solves_per_s': len(done) / wall if wall > 0 else 0.0,
                 'p50_ms': float(np.percentile(lat, 50) * 1e3),
                 'p99_ms': float(np.percentile(lat, 99) * 1e3),
-                'max_err': float(max([r.error for r in done], default=0.0)),
+                'max_residual': float(max([r.error for r in done], default=0.0)),
                 'device_bytes': self.used_bytes}
 
 

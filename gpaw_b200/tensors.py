@@ -55,6 +55,11 @@ def stream_of(t):
     return torch.cuda.current_stream(t.device).cuda_stream
 
 
+def stream_of_device(device):
+    """The current stream of a CUDA device (torch.device or index)."""
+    return torch.cuda.current_stream(device).cuda_stream
+
+
 def nbands(t):
     """Number of 3-D arrays in a (..., n0, n1, n2) tensor."""
     n = 1

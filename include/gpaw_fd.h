@@ -45,6 +45,7 @@ extern "C" {
 #define GFD_ETIMEOUT 4    /* a bounded device-side wait ran out */
 #define GFD_ECUDA 5       /* a CUDA runtime call failed */
 #define GFD_EUNSUPPORTED 6 /* valid in the reference but not provided here */
+#define GFD_ENEEDGAUSS 7  /* charged non-periodic solve before gfd_poisson_load_gauss */
 
 /* Element types (the `dtype` argument).  The FP32 types are the reduced-
  * precision variants; the reference computes in float64 / complex128 only. */
@@ -186,6 +187,20 @@ GFD_API int gfd_density_interpolate(gfd_transformer* tr, const double* nt_sG, do
  * kernels have no such waits. */
 GFD_API int gfd_device_errors(int* flags);
 
+/* Fault injection for tests of the out-of-memory paths (no counterpart in
+ * the reference, whose GPAW_MALLOC aborts): n > 0 makes the n-th device
+ * allocation the library makes from now on fail with GFD_ENOMEM, without
+ * touching the device; 0 cancels a planned failure.  Host-side only. */
+GFD_API int gfd_test_fail_alloc(long long n);
+
+/* Self-test of the bounded waits behind gfd_device_errors (no counterpart in
+ * the reference): one small kernel waits, with the stencil kernels' bounded
+ * mbarrier wait limited to max_cycles SM cycles (1 .. about 4e9), on a
+ * barrier that nothing completes, sets the device error flag when the wait
+ * runs out and returns; nothing is copied, so the early exit leaves no work
+ * in flight.  Waits for the device.  gfd_device_errors then reports 1. */
+GFD_API int gfd_wait_selftest(long long max_cycles);
+
 /* ------------------------------------------------------------------------
  * Grid transformer (restriction / interpolation).
  * Replaces _gpaw.Transformer(size_in, size_out, k, paddings, npaddings,
@@ -236,18 +251,52 @@ GFD_API int gfd_poisson_destroy(gfd_poisson* ps);
  * previous form. */
 GFD_API int gfd_poisson_set_rhs_operator(gfd_poisson* ps, gfd_operator* B);
 
-/* PoissonSolver.solve(phi, rho, charge=None, eps, maxcharge) for a charge-
- * neutral rho (gpaw/poisson.py:124-138, 193-218).  phi (in: initial guess,
- * out: solution) and rho are device float64 arrays of the fine grid.
- * charge: pass NaN for None (the integral of rho is used).  When
- * |charge| > maxcharge the call returns GFD_EUNSUPPORTED (the charged
- * branches are outside this library).  maxiter = 1000 in the reference.
+/* PoissonSolver.solve(phi, rho, charge=None, eps, maxcharge)
+ * (gpaw/poisson.py:124-218).  phi (in: initial guess, out: solution) and rho
+ * are device float64 arrays of the fine grid.  charge: pass NaN for None
+ * (the integral of rho is used).  maxiter = 1000 in the reference.
+ *   |charge| <= maxcharge: the neutral solve of rho - background.
+ *   charged, every axis periodic: the neutral solve shifted by
+ *     charge * madelung (gfd_poisson_set_madelung; GFD_EUNSUPPORTED if unset).
+ *   charged, no axis periodic: the monopole (the integral of rho) is carried
+ *     by the L = 0 Gaussian of gfd_poisson_load_gauss, whose potential is
+ *     added back; GFD_ENEEDGAUSS, with phi unchanged, if it is not loaded.
+ *   charged, mixed boundary conditions: GFD_EUNSUPPORTED (the reference
+ *     raises NotImplementedError).
  * On return (the call waits for the stream) *niter holds the V-cycle count
  * and *error the last residual norm sum(r^2) dv; GFD_ENOCONV when
  * niter reached maxiter, as PoissonConvergenceError. */
 GFD_API int gfd_poisson_solve(gfd_poisson* ps, double* phi, const double* rho, double charge,
                       double eps, double maxcharge, int maxiter, int* niter, double* error,
                       void* stream);
+/* The same with flags: GFD_SOLVE_ZERO_INITIAL_PHI is the reference's
+ * zero_initial_phi=True -- the charged branches start from phi = 0 instead
+ * of the shifted guess; the neutral branch keeps phi as given, as in the
+ * reference (gpaw/poisson.py:124-138). */
+#define GFD_SOLVE_ZERO_INITIAL_PHI 1
+GFD_API int gfd_poisson_solve_ex(gfd_poisson* ps, double* phi, const double* rho, double charge,
+                                 double eps, double maxcharge, int maxiter, int flags,
+                                 int* niter, double* error, void* stream);
+
+/* The compensating Gaussian of the charged non-periodic branch: Poisson-
+ * Solver.load_gauss (gpaw/poisson.py:118-123) with Gaussian(gd).get_gauss(0)
+ * and get_gauss_pot(0) (gpaw/utilities/gauss.py:47-82):
+ *   g(r) = sqrt(4 a^3) / pi exp(-a r^2),  v(r) = 2 sqrt(pi) erf(sqrt(a) r) / r,
+ * r the distance of grid point i (coordinates (i + beg_c) h_cv) from
+ * center_v, r^2 clamped to at least 1e-12 (gpaw/utilities/tools.py:92-118).
+ * The reference's a = 4 * 19 * max_c sum_v icell_cv^2 and center_v = half
+ * the cell's diagonal.  Computed on the device into two level-0 arrays the
+ * solver owns; the call waits for the stream. */
+GFD_API int gfd_poisson_load_gauss(gfd_poisson* ps, const double h_cv[9], const int64_t beg_c[3],
+                                   const double center_v[3], double a, void* stream);
+/* Potential shift per unit charge of the charged periodic branch
+ * (charged_periodic_correction = madelung(cell_cv), gpaw/poisson.py:143-151). */
+GFD_API int gfd_poisson_set_madelung(gfd_poisson* ps, double madelung);
+/* madelung(cell_cv) of gpaw/utilities/ewald.py:148: the Ewald potential at a
+ * probe charge -1 from its periodic images in a neutralising background
+ * (G = 5 / longest lattice vector, 9^3 reciprocal and 3^3 real-space shells
+ * either side), computed on the host. */
+GFD_API int gfd_madelung(const double cell_cv[9], double* out);
 
 /* Asynchronous form of gfd_poisson_solve for callers that keep several solves
  * in flight (serving).  Enqueues the whole solve on `stream` -- copies of
@@ -326,7 +375,8 @@ GFD_API int gfd_poisson_batch_grouped(const gfd_poisson_batch* batch, int* group
 typedef struct gfd_tune_plan {
   int form;         /* 0: one thread per point; 1: marching kernel */
   int tile;         /* marching tile: 0 32 columns, 1 16, 2 8, 3 32 columns x 8 rows,
-                       4 complex bands with re / im on lane pairs (radius <= 3) */
+                       4 complex bands with re / im on lane pairs (radius <= 3),
+                       5 the same for complex128 on full rows staged by TMA */
   int ctas_per_sm;  /* axis-0 split target */
   double us;        /* measured time per launch, microseconds */
 } gfd_tune_plan;

@@ -144,9 +144,12 @@ def test_grouped_batch_with_large_grids(cuda):
 
 
 def test_grouped_batch_charged_and_maxiter(cuda):
-    """Per-solve outcomes inside one grouped launch: a charged request is
-    refused (NotImplementedError) without touching the others, and maxiter
-    stops every solve at that count (PoissonConvergenceError)."""
+    """Per-solve outcomes inside one grouped launch: a charged zero-boundary
+    request whose solver has not loaded the compensating Gaussian is refused
+    (NotImplementedError, phi untouched) without touching the others; once
+    that solver loads it, the same launch solves the charged request as a
+    solve alone does.  maxiter stops every solve at that count
+    (PoissonConvergenceError)."""
     import torch
     from gpaw_b200.errors import PoissonConvergenceError
     sizes = [32, 32, 32]
@@ -156,11 +159,19 @@ def test_grouped_batch_charged_and_maxiter(cuda):
     phis = [torch.zeros_like(r) for r in rhos]
     with pytest.raises(NotImplementedError):
         batch.solve(phis, rhos)
+    assert not phis[1].any()
     for i in (0, 2):
         n, err = solvers[i].result()
         phi, n_alone = solve_alone(cuda, sizes[i], rhos[i])
         assert n == n_alone and err <= 2e-10
         assert torch.equal(phi, phis[i])
+    solvers[1].load_gauss()
+    phis = [torch.zeros_like(r) for r in rhos]
+    res = batch.solve(phis, rhos)
+    phi, n_alone = solve_alone(cuda, sizes[1], rhos[1])
+    assert res[1][0] == n_alone and torch.equal(phi, phis[1])
+    phi_o, n_o = oracle_solve(sizes[1], rhos[1].cpu().numpy())
+    assert n_alone == n_o and np.abs(phi.cpu().numpy() - phi_o).max() < 1e-10
     rhos[1] = rhos[1] - rhos[1].mean()
     phis = [torch.zeros_like(r) for r in rhos]
     with pytest.raises(PoissonConvergenceError):
@@ -246,3 +257,76 @@ def test_server_memory_budget_rejects(cuda):
     reqs = [Request(0, 32, 0.0, rho)]
     stats = srv.run(reqs)
     assert stats['rejected'] == 1 and reqs[0].status.startswith('rejected')
+
+
+def test_server_deadline_and_cancel(cuda):
+    """Host-side request failures: with one launch in flight at a time, the
+    requests queued behind it with a zero admission deadline expire; a
+    request cancelled before it arrives never runs, one cancelled right after
+    the start is dropped whether it still waits or already runs (its result
+    discarded); the other requests finish and equal their solves alone."""
+    import torch
+    from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
+    sizes = [64] * 8
+    rhos = [pair_density(grid_for(N, H, device=cuda), 50 + i) for i, N in enumerate(sizes)]
+    torch.cuda.synchronize()
+    srv = PoissonServer(H, max_inflight=1, nstreams=2, device=cuda, keep_results=True, slots=1)
+    reqs = [Request(i, N, 0.0, rhos[i]) for i, N in enumerate(sizes)]
+    for r in reqs[5:7]:
+        r.deadline = 0.0                      # must be admitted at once: they cannot be
+    reqs[3].arrival, reqs[3].cancel_at = 0.5, 0.0   # cancelled before it arrives
+    reqs[1].cancel_at = 1e-4                  # cancelled right after the start
+    stats = srv.run(reqs)
+    assert [r.status for r in reqs[5:7]] == ['expired', 'expired']
+    assert reqs[3].status == 'cancelled' and reqs[3].admit is None
+    assert reqs[1].status == 'cancelled' and reqs[1].phi is None
+    assert stats['expired'] == 2 and stats['cancelled'] == 2
+    for i in (0, 2, 4, 7):
+        assert reqs[i].status == 'ok'
+        phi, n = solve_alone(cuda, sizes[i], rhos[i])
+        assert reqs[i].niter == n and torch.equal(reqs[i].phi, phi)
+
+
+def test_server_device_allocation_failure(cuda):
+    """A failing device allocation (planned through gfd_test_fail_alloc, on
+    the host): the pod cannot be created, the request is rejected with
+    nothing in flight, and the server goes on to serve the next requests.
+    The same planned failure surfaces as MemoryError from the solver, the
+    relaxation scratch and the preconditioner."""
+    import torch
+    from gpaw_b200 import _lib
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.poisson import PoissonSolver
+    from gpaw_b200.preconditioner import Preconditioner
+    from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
+    rho = pair_density(grid_for(32, H, device=cuda), 5)
+    torch.cuda.synchronize()
+    srv = PoissonServer(H, device=cuda, keep_results=True, slots=1)
+    try:
+        assert _lib.lib.gfd_test_fail_alloc(1) == 0
+        stats = srv.run([Request(0, 32, 0.0, rho)])
+        assert stats['rejected'] == 1 and srv.alloc_failures == 1
+        reqs = [Request(1, 32, 0.0, rho), Request(2, 32, 0.0, rho)]
+        stats = srv.run(reqs)
+        assert stats['completed'] == 2 and all(r.status == 'ok' for r in reqs)
+        phi, n = solve_alone(cuda, 32, rho)
+        assert torch.equal(reqs[0].phi, phi)
+
+        gd = grid_for(40, H, device=cuda)
+        ps = PoissonSolver(3, 'J', 2e-10)
+        ps.set_grid_descriptor(gd)
+        assert _lib.lib.gfd_test_fail_alloc(1) == 0
+        with pytest.raises(MemoryError):
+            ps.initialize()
+        ps.initialize()                       # the next allocation succeeds
+        lap = Laplace(gd, -0.25 / np.pi, 3)
+        f = torch.zeros(tuple(int(x) for x in gd.n_c), dtype=torch.float64, device=cuda)
+        assert _lib.lib.gfd_test_fail_alloc(1) == 0
+        with pytest.raises(MemoryError):
+            lap.relax(2, f, f.clone(), 1, 1.0)
+        kin = Laplace(gd, -0.5, 3, complex)
+        assert _lib.lib.gfd_test_fail_alloc(1) == 0
+        with pytest.raises(MemoryError):
+            Preconditioner(gd, kin, complex, block=2)
+    finally:
+        _lib.lib.gfd_test_fail_alloc(0)

@@ -300,7 +300,7 @@ def test_pseudo_hamiltonian_fused(cuda, case):
     import torch
     from gpaw_b200.fd_operators import FDOperator
     from gpaw_b200.grid_descriptor import GridDescriptor
-    from gpaw_b200.hamiltonian import apply_pseudo_hamiltonian
+    from gpaw_b200.fd_operators import apply_pseudo_hamiltonian
     rng = np.random.default_rng(31)
     if case == 'bloch96':
         gd = G.Grid((96,) * 3, (96 * 0.18 / BOHR,) * 3, 1)
@@ -369,3 +369,52 @@ def test_host_streamer_matches_device_apply(cuda):
     assert rel_err(host_out.numpy(), host(ref)) < TOL
     with pytest.raises(ValueError):
         st.apply(t, ref, ph)  # device tensors
+
+
+@pytest.mark.parametrize('switches', [{'GFD_TMASPLIT': '0'},
+                                      {'GFD_TMASPLIT': '0', 'GFD_SPLIT': '0'}])
+def test_other_complex_kernels_in_subprocess(cuda, switches):
+    """complex128 bands up to radius 3 take the TMA-staged lane-pair kernel
+    (star_tmasplit_kernel) where it applies; GFD_TMASPLIT=0 (read once per
+    process) moves them to the cp.async lane-pair kernel (star_split_kernel,
+    also the complex64 kernel), and GFD_SPLIT=0 as well to star_kernel.  The
+    complex tests above, the pseudo-Hamiltonian and the preconditioner in a
+    child process with the switches, so every kernel stays checked against
+    the oracle."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, **switches)
+    r = subprocess.run([sys.executable, '-m', 'pytest', '-q', '-m', 'gpu', '-p', 'no:cacheprovider',
+                        os.path.join(root, 'tests', 'test_gpu_stencil.py'),
+                        os.path.join(root, 'tests', 'test_gpu_preconditioner.py'),
+                        '-k', 'complex128_tiles or bloch_complex_96 or register_blocked or '
+                              'pseudo_hamiltonian or preconditioner'],
+                       cwd=root, env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert ' passed' in r.stdout
+
+
+def test_bounded_wait_runs_out_and_reports(cuda):
+    """The kernels' bounded mbarrier wait, made to run out: a probe kernel
+    waits (limit 100000 SM cycles) on a barrier nothing completes, returns,
+    and gfd_device_errors reports the flag once and then reads clear; the
+    context stays usable (a stencil apply afterwards matches the oracle)."""
+    import ctypes
+    from gpaw_b200 import _lib
+    flags = ctypes.c_int(-1)
+    assert _lib.lib.gfd_device_errors(ctypes.byref(flags)) == 0  # clear any earlier flag
+    assert _lib.lib.gfd_wait_selftest(100000) == _lib.GFD_OK, _lib.last_error()
+    assert _lib.lib.gfd_device_errors(ctypes.byref(flags)) == 0
+    assert flags.value == 1
+    assert _lib.lib.gfd_device_errors(ctypes.byref(flags)) == 0
+    assert flags.value == 0
+    assert _lib.lib.gfd_wait_selftest(0) == _lib.GFD_EINVAL
+    gd = G.Grid((20, 16, 40), np.array((20, 16, 40)) * 0.3, 1)
+    c, o = G.laplace_stencil(gd, -0.5, 3)
+    rng = np.random.default_rng(2)
+    a = rng.standard_normal((1,) + tuple(gd.n_c)) + 1j * rng.standard_normal((1,) + tuple(gd.n_c))
+    ph = G.bloch_phases(gd, (0.2, 0.1, -0.3))
+    args = (gd.N_c, gd.cell_cv, gd.pbc_c)
+    assert rel_err(gpu_apply(cuda, args, c, o, a, ph), K.fd_apply(c, o, gd.pbc_c, a, ph)) < TOL

@@ -207,3 +207,16 @@ def test_tune_cache_file_roundtrip(tmp_path):
     assert lib.gfd_autotune_count(ctypes.byref(n)) == 0 and n.value == 2
     assert lib.gfd_autotune_clear() == 0
     assert lib.gfd_autotune_count(ctypes.byref(n)) == 0 and n.value == 0
+
+
+def test_madelung_matches_oracle():
+    """gfd_madelung (host code of the library) against the oracle's
+    restatement of gpaw/utilities/ewald.py:148, and the simple cubic
+    lattice's known value in a neutralising background, 2.837297 / L."""
+    from gpaw_b200.poisson import madelung
+    from oracle import poisson as OP
+    for cell in (np.diag([10.0, 10.0, 10.0]), np.diag([9.0, 12.0, 15.5]),
+                 np.array([[8.0, 0.0, 0.0], [2.0, 9.0, 0.0], [0.5, 1.0, 11.0]])):
+        m = madelung(cell)
+        assert abs(m - OP.madelung(cell)) < 1e-12 * abs(m), cell
+    assert abs(madelung(np.diag([7.3] * 3)) * 7.3 - 2.837297) < 1e-6
