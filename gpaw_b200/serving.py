@@ -262,10 +262,12 @@ class PoissonServer:
         return pod
 
     # -- serving loop ----------------------------------------------------------
-    def run(self, requests):
+    def run(self, requests, metrics=None):
         """Serve `requests` (Request objects with arrival times in seconds from
         the start of the run).  Returns a summary dict; per-request results are
-        stored on the Request objects."""
+        stored on the Request objects.  `metrics` (a timing.MetricsLog): one
+        'request' record per request and one 'summary' record are written
+        after the run, so that logging does not slow the serving loop."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         queues = collections.OrderedDict()   # N -> arrived requests, not admitted
         # Work on one stream completes in order, so only the oldest launch of
@@ -360,7 +362,7 @@ class PoissonServer:
         wall = time.perf_counter() - t0
         done = [r for r in requests if r.status == 'ok']
         lat = np.array([r.done - r.arrival for r in done]) if done else np.zeros(1)
-        return {'requests': len(requests), 'completed': len(done),
+        summary = {'requests': len(requests), 'completed': len(done),
                 'rejected': self.rejected - rejected0,
                 'expired': sum(r.status == 'expired' for r in requests),
                 'cancelled': sum(r.status == 'cancelled' for r in requests),
@@ -371,6 +373,13 @@ class PoissonServer:
                 'p99_ms': float(np.percentile(lat, 99) * 1e3),
                 'max_residual': float(max([r.error for r in done], default=0.0)),
                 'device_bytes': self.used_bytes}
+        if metrics is not None:
+            for r in requests:
+                metrics.log('request', rid=r.rid, N=r.N, arrival_s=r.arrival, admit_s=r.admit,
+                            done_s=r.done, status=r.status, niter=r.niter, residual=r.error)
+            metrics.log('summary', precision=self.precision, **summary)
+            metrics.flush()
+        return summary
 
 
 def pair_density(gd, seed, ngauss=8):

@@ -330,3 +330,53 @@ def test_server_device_allocation_failure(cuda):
             Preconditioner(gd, kin, complex, block=2)
     finally:
         _lib.lib.gfd_test_fail_alloc(0)
+
+
+def test_server_metrics_and_cuda_timer(cuda):
+    """The JSON-lines stream of a served run has one record per request,
+    carrying its status and V-cycle count, and a summary equal to the
+    returned one; a CudaTimer around solves reports device time for the
+    nested regions (positive, outer >= inner)."""
+    import io
+    import json
+    import torch
+    from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
+    from gpaw_b200.timing import CudaTimer, MetricsLog
+    rhos = [pair_density(grid_for(32, H, device=cuda), 70 + i) for i in range(4)]
+    srv = PoissonServer(H, device=cuda, slots=2, nstreams=2)
+    reqs = [Request(i, 32, 0.0, rhos[i]) for i in range(4)]
+    buf = io.StringIO()
+    stats = srv.run(reqs, metrics=MetricsLog(buf))
+    recs = [json.loads(line) for line in buf.getvalue().splitlines()]
+    per = [r for r in recs if r['kind'] == 'request']
+    assert sorted(r['rid'] for r in per) == [0, 1, 2, 3]
+    for r, q in zip(sorted(per, key=lambda r: r['rid']), reqs):
+        assert r['status'] == 'ok' and r['niter'] == q.niter and r['done_s'] >= r['arrival_s']
+    summ = [r for r in recs if r['kind'] == 'summary']
+    assert len(summ) == 1 and summ[0]['completed'] == stats['completed'] == 4
+
+    timer = CudaTimer()
+    ps, phi = solve_timer_setup(cuda, rhos[0])
+    timer.start('Poisson')
+    for _ in range(3):
+        timer.start('solve')
+        phi.zero_()
+        ps.solve(phi, rhos[0])
+        timer.stop('solve')
+    timer.stop('Poisson')
+    outer, inner = timer.get_time('Poisson'), timer.get_time('Poisson', 'solve')
+    assert 0 < inner <= outer
+    buf = io.StringIO()
+    MetricsLog(buf).timer(timer)
+    regions = {json.loads(line)['region'] for line in buf.getvalue().splitlines()}
+    assert {'Poisson', 'Poisson.solve', 'Other', 'Total'} <= regions
+
+
+def solve_timer_setup(cuda, rho):
+    import torch
+    from gpaw_b200.poisson import PoissonSolver
+    from gpaw_b200.serving import grid_for
+    ps = PoissonSolver(3, 'J', 2e-10)
+    ps.set_grid_descriptor(grid_for(32, H, device=cuda))
+    ps.initialize()
+    return ps, torch.zeros_like(rho)

@@ -220,3 +220,42 @@ def test_madelung_matches_oracle():
         m = madelung(cell)
         assert abs(m - OP.madelung(cell)) < 1e-12 * abs(m), cell
     assert abs(madelung(np.diag([7.3] * 3)) * 7.3 - 2.837297) < 1e-6
+
+
+def test_timer_nesting_and_metrics_log(tmp_path):
+    """Timer keeps the reference's rules (gpaw/utilities/timing.py:86-166):
+    regions nest by name, stop must follow stack order, inclusive and
+    exclusive times add up; MetricsLog writes one JSON object per line."""
+    import json
+    import time
+    from gpaw_b200.timing import MetricsLog, Timer
+    t = Timer()
+    t.start('SCF')
+    t.start('Poisson')
+    time.sleep(0.02)
+    with pytest.raises(RuntimeError, match='stack order'):
+        t.stop('SCF')
+    t.stop('Poisson')
+    t.start('Poisson')
+    time.sleep(0.01)
+    t.stop()
+    t.stop('SCF')
+    with pytest.raises(RuntimeError):
+        t.stop()
+    scf, poisson = t.get_time('SCF'), t.get_time('SCF', 'Poisson')
+    assert 0.03 <= poisson <= scf
+    rows, tot = t.table()
+    excl = {names: te for names, _, te in rows}
+    assert abs(excl[('SCF',)] - (scf - poisson)) < 1e-12
+    assert abs(sum(excl.values()) - tot) < 1e-9
+    u = Timer()
+    u.add(t)
+    u.add(t)
+    assert abs(u.get_time('SCF', 'Poisson') - 2 * poisson) < 1e-12
+    path = str(tmp_path / 'm.jsonl')
+    with MetricsLog(path) as m:
+        m.log('request', rid=1, N=np.int64(32), residual=np.float64(1e-11), status='ok')
+        m.timer(t)
+    recs = [json.loads(line) for line in open(path)]
+    assert recs[0]['kind'] == 'request' and recs[0]['N'] == 32 and recs[0]['residual'] == 1e-11
+    assert [r['region'] for r in recs[1:]] == ['SCF', 'SCF.Poisson', 'Other', 'Total']
