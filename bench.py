@@ -371,19 +371,22 @@ def serving_bench(rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), nreq=10000,
             last = lam == rates[-1]
             srv.keep_results = False
             srv.run([Request(-1, r.N, 0.0, r.rho) for r in reqs[:16]])  # warm (not timed)
+            picked = collections.defaultdict(list)
             if check and last:
-                srv.keep_results = True
+                # the sample: the first two requests of each size up to 96^3;
+                # only their potentials are copied out during the run
+                for r in reqs:
+                    if r.N <= 96 and len(picked[r.N]) < 2:
+                        picked[r.N].append(r)
+                ids = {r.rid for rs in picked.values() for r in rs}
+                srv.keep_results = lambda r: r.rid in ids
             stats = srv.run(reqs)
             res['%g/s' % lam] = {k: stats[k] for k in (
                 'requests', 'completed', 'solves_per_s', 'wall_s', 'p50_ms', 'p99_ms',
                 'max_residual', 'rejected', 'expired', 'cancelled', 'failed')}
             if check and last:
-                picked = collections.defaultdict(list)
-                for r in reqs:
-                    if r.N <= 96 and r.status == 'ok' and len(picked[r.N]) < 2:
-                        picked[r.N].append(r)
                 sample[prec] = [(r.N, r.rho, r.phi.cpu().numpy())
-                                for N in picked for r in picked[N]]
+                                for N in picked for r in picked[N] if r.status == 'ok']
             srv.keep_results = False
         res['device_bytes'] = srv.used_bytes
         out[prec] = res

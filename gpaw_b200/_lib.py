@@ -47,7 +47,8 @@ class TunePlan(ctypes.Structure):
     """gfd_tune_plan: form 0 one thread per point / 1 marching kernel, the
     marching tile (0: 32 columns, 1: 16, 2: 8, 3: 32 columns by 8 rows, 4: complex
     bands with the real and imaginary parts on lane pairs, 5: the same for
-    complex128 on full rows staged by TMA), the
+    complex128 on full rows staged by TMA, 6: complex128, 48 columns by 8
+    rows), the
     axis-0 split target in CTAs per SM and the measured microseconds per
     launch."""
     _fields_ = [('form', ctypes.c_int), ('tile', ctypes.c_int), ('ctas_per_sm', ctypes.c_int),
@@ -55,7 +56,7 @@ class TunePlan(ctypes.Structure):
 
     def as_dict(self):
         return {'form': ('direct', 'march')[self.form],
-                'tile': (32, 16, 8, '32x8', 'split', 'tma-split')[self.tile],
+                'tile': (32, 16, 8, '32x8', 'split', 'tma-split', '48x8')[self.tile],
                 'ctas_per_sm': self.ctas_per_sm, 'us': self.us}
 
 # Every function the header declares: name -> (restype, argtypes).

@@ -59,7 +59,7 @@ int per_mask(const int per[3]) { return (per[0] ? 1 : 0) | (per[1] ? 2 : 0) | (p
 
 bool plan_valid(const TunePlan& p) {
   return (p.path == PLAN_DIRECT || p.path == PLAN_MARCH) && p.tile >= TILE_WIDE &&
-         p.tile <= TILE_TMASPLIT && p.cps >= 1 && p.cps <= 64;
+         p.tile <= TILE_48 && p.cps >= 1 && p.cps <= 64;
 }
 
 int load_file(const char* path);
@@ -257,6 +257,9 @@ extern "C" int gfd_autotune_operator(gfd_operator* op, int dtype, int mode, cons
     tiles.push_back(TILE_SHORT);
   if (dtype_is_complex(dtype) && op->R <= 3) tiles.push_back(TILE_SPLIT);
   if (dtype == GFD_COMPLEX128 && op->R <= 3) tiles.push_back(TILE_TMASPLIT);
+  if (dtype == GFD_COMPLEX128 && (imode == OP_APPLY || imode == OP_POTENTIAL) &&
+      tile48_eligible(op))
+    tiles.push_back(TILE_48);
   const std::vector<TunePlan> cands = march_candidates(tiles);
   const double* ph = dtype_is_complex(dtype) ? phase_cd : nullptr;
   TunePlan pick;

@@ -72,6 +72,36 @@ __device__ __forceinline__ cplx<S> phase_mul(const cplx<S>& p, const cplx<S>& v)
   return cmul(p, v);
 }
 
+// Asynchronous global->shared copies (sm_80+ cp.async).  A source size of 0
+// writes zeros (zero boundary points); the source address is then unused but
+// kept valid.  16-byte copies use the L1-allocating form (.ca): measured on
+// B200, the cache-bypass form (.cg) fetched one 32-byte L2 sector per lane
+// and wrote shared memory one lane at a time (about 28 shared-store
+// wavefronts per warp copy of 512 contiguous bytes, against 4.5 for .ca), so
+// it moved twice the bytes from L2.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid) {
+  const unsigned d = smem_addr(dst);
+  const int n = valid ? BYTES : 0;
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
+                 "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Read-only global loads (one vector instruction per element).
 __device__ __forceinline__ double ldro(const double* p) { return __ldg(p); }
 __device__ __forceinline__ float ldro(const float* p) { return __ldg(p); }

@@ -55,19 +55,27 @@ int num_sms();
 // the cached plan when there is one and the built-in rules otherwise.
 // ---------------------------------------------------------------------------
 // Marching tiles 32 / 16 / 8 columns wide; TILE_SHORT: 32 columns by 8 rows
-// (complex128 apply up to radius 4 only: 128 threads, four CTAs per SM).
+// (complex128 apply up to radius 4 only: 128 threads, three CTAs per SM).
 // TILE_SPLIT: complex bands, radius <= 3, real and imaginary parts on lane
 // pairs (star_split_kernel): 32 columns by 16 rows, 128 threads.
 // TILE_TMASPLIT: complex128, radius <= 3, the same lane pairs on full-row
 // tiles of 8 rows staged by TMA (star_tmasplit_kernel).
+// TILE_48: complex128 apply (and apply with a potential) up to radius 4,
+// 48 columns by 8 rows (48 x 4 threads, 2 rows each, two CTAs per SM), for
+// axis-2 lengths that are multiples of 48: it stages 2R halo columns per 48
+// where the 32-column tiles stage 2R per 32.
 enum {
   TILE_WIDE = 0,
   TILE_MID = 1,
   TILE_NARROW = 2,
   TILE_SHORT = 3,
   TILE_SPLIT = 4,
-  TILE_TMASPLIT = 5
+  TILE_TMASPLIT = 5,
+  TILE_48 = 6
 };
+inline bool tile48_eligible(const gfd_operator* op) {
+  return op->star && op->R >= 1 && op->R <= 4 && op->n[2] % 48 == 0;
+}
 enum { PLAN_DIRECT = 0, PLAN_MARCH = 1 };               // one thread per point / marching
 enum { TK_STAR = 0, TK_RESTRICT = 1, TK_INTERP = 2 };
 

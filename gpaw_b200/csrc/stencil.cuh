@@ -51,36 +51,6 @@ struct StarParams {
   const void* pot;  // MODE_POTENTIAL: real potential v (one grid, type S)
 };
 
-// Asynchronous global->shared copies (sm_80+ cp.async).  A source size of 0
-// writes zeros (zero boundary points); the source address is then unused but
-// kept valid.  16-byte copies use the L1-allocating form (.ca): measured on
-// B200, the cache-bypass form (.cg) fetched one 32-byte L2 sector per lane
-// and wrote shared memory one lane at a time (about 28 shared-store
-// wavefronts per warp copy of 512 contiguous bytes, against 4.5 for .ca), so
-// it moved twice the bytes from L2.
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid) {
-  const unsigned d = smem_addr(dst);
-  const int n = valid ? BYTES : 0;
-  if constexpr (BYTES == 16)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n)
-                 : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
-                 "r"(n)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // Block-wide sum of one double per thread in a fixed order.
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -123,11 +93,17 @@ constexpr size_t star_smem_bytes() {
 //    c0' = -(1-w) c0 / w, which equals (1-w) phi + w (rho - sum) / c0.
 //  * The source term of MODE_JACOBI / MODE_RESIDUAL travels in the same
 //    pipeline stages.
-// The short tile (32 x 4 threads, 2 rows each) is meant to run four CTAs
-// per SM (128 registers).
+// CTAs per SM the register allocation is sized for: the short tile
+// (32 x 4 threads, 2 rows each) and the 48-column tile (48 x 4 threads,
+// 2 rows each), both for complex128 apply up to radius 4.  Measured on the
+// 512-band 96^3 complex128 Laplace: the short tile at 3 CTAs per SM (up to
+// 170 registers) 3934 GB/s against 3744 at 4 (128 registers, the limit
+// there) and 3232 at 2; the 48-column tile at 2 per SM 4010-4099, at 3
+// (spilling) 2770.
+constexpr int kShortTileZ = 32, kTile48Z = 48;
 template <int BZ, int TY, int VY>
 constexpr int star_min_ctas() {
-  return BZ == 32 && TY == 4 && VY == 2 ? 4 : 1;
+  return TY == 4 && VY == 2 ? (BZ == kShortTileZ ? 3 : (BZ == kTile48Z ? 2 : 1)) : 1;
 }
 
 template <class V, int R, int BZ, int TY, int VY, int S, int MODE>

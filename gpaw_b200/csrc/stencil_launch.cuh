@@ -34,6 +34,7 @@ inline TileDims tile_dims(int tile) {
     case TILE_MID: return {16, 16, 128};
     case TILE_SHORT: return {32, 8, 128};
     case TILE_SPLIT: return {32, 4 * GFD_SPLIT_VY, 128};
+    case TILE_48: return {kTile48Z, 8, 4 * kTile48Z};
     default: return {32, 16, 128};
   }
 }
@@ -92,11 +93,10 @@ void fill_phases(Phases<S>& P, const double* ph) {
     }
 }
 
-template <class V, int R, int BZ, int TY, int VY, int MODE>
+template <class V, int R, int BZ, int TY, int VY, int MODE, int S = kStages>
 int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t nin,
             const StarParams<typename vt<V>::S>& base, const LaunchGeom& g, double* partials,
             cudaStream_t s) {
-  constexpr int S = kStages;
   constexpr size_t smem = star_smem_bytes<BZ, TY, VY, R, S, V, MODE>();
   auto kern = star_kernel<V, R, BZ, TY, VY, S, MODE>;
   int st = raise_smem_limit(kern, smem, "cudaFuncSetAttribute(star_kernel)");
@@ -121,17 +121,26 @@ int star_go(const gfd_operator* op, const V* in, V* out, const V* rho, int64_t n
 constexpr int kMaxComplexRelaxR = 3;
 
 // The short tile exists for complex128 apply (and apply with a potential)
-// up to radius 4 (beyond, its 2R + 1 partial sums per row do not fit 128
-// registers).  It is the built-in choice for those launches: four CTAs of
-// 128 threads per SM measured fastest on B200 (the 512-band 96^3 Laplace:
-// 3730 GB/s against 3120 for the 32 x 16 tile, 3100 for the lane-pair
-// kernel and 3270 for its TMA-staged form, one box, 16-byte cp.async in the
-// L1-allocating form).
+// up to radius 4 (beyond, its 2R + 1 partial sums per row do not fit the
+// registers of three CTAs per SM).  It is the built-in choice for those
+// launches where the 48-column tile below does not apply: on B200 (the
+// 512-band 96^3 Laplace, one box) it measured 3730 GB/s at four CTAs of 128
+// threads per SM, against 3120 for the 32 x 16 tile, 3100 for the lane-pair
+// kernel and 3270 for its TMA-staged form; three CTAs per SM with up to 170
+// registers took it to 3934.
 constexpr int kMaxShortR = 4;
 template <class V, int R, int MODE>
 constexpr bool has_short_tile() {
   return sizeof(V) >= 16 && (MODE == MODE_APPLY || MODE == MODE_POTENTIAL) && R <= kMaxShortR;
 }
+// The 48-column tile (TILE_48) covers the same launches where axis 2 is a
+// multiple of 48 and is then the built-in choice: 48 x 4 threads with 2
+// rows each, two CTAs per SM.  On the 512-band 96^3 Laplace it measured
+// 4010-4099 GB/s against 3730-3826 for the short tile at 4 CTAs per SM
+// (3934 at 3)
+// (apply with a potential: 3610-3750 against 3260-3380).  A 96-column tile
+// measured slower at every thread shape tried (2110-3570 GB/s): one CTA per
+// SM, or registers short of its 2R + 1 partial sums per row.
 
 template <class V, int R, int MODE>
 int star_wide(const gfd_operator* op, int tile, const V* in, V* out, const V* rho, int64_t nin,
@@ -140,6 +149,8 @@ int star_wide(const gfd_operator* op, int tile, const V* in, V* out, const V* rh
   if constexpr (has_short_tile<V, R, MODE>()) {
     if (tile == TILE_SHORT)
       return star_go<V, R, 32, 4, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
+    if (tile == TILE_48)
+      return star_go<V, R, kTile48Z, 4, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
   }
   if constexpr (sizeof(V) >= 16 || R > 3)
     return star_go<V, R, 32, 8, 2, MODE>(op, in, out, rho, nin, p, g, partials, s);
@@ -431,10 +442,12 @@ int launch_star_typed(const gfd_operator* op, int mode, const void* in, void* ou
   const bool tsplit = ts_eligible<V>(op, mode, in, rho);
   const bool shortok =
       sizeof(V) >= 16 && (mode == OP_APPLY || mode == OP_POTENTIAL) && op->R <= kMaxShortR;
-  if (shortok && tile == TILE_WIDE) tile = TILE_SHORT;
+  if (shortok && tile == TILE_WIDE) tile = tile48_eligible(op) ? TILE_48 : TILE_SHORT;
   if (tuned) {
     if (plan.tile == TILE_SHORT)
       tile = shortok ? TILE_SHORT : tile;
+    else if (plan.tile == TILE_48)
+      tile = shortok && tile48_eligible(op) ? TILE_48 : tile;
     else if (plan.tile == TILE_TMASPLIT)
       tile = tsplit ? TILE_TMASPLIT : tile;
     else if (plan.tile == TILE_SPLIT)

@@ -143,8 +143,9 @@ class Request:
 class _Pod:
     """`slots` solvers of one grid size that launch together: one graph
     launch (a PoissonBatch) serves up to `slots` requests; `phis` are the
-    slots' potential buffers."""
-    __slots__ = ('N', 'solvers', 'batch', 'nbytes', 'phis')
+    slots' potential buffers.  `ready`: an event that the pod's next launch
+    must wait for (the copies of its last results, when they are kept)."""
+    __slots__ = ('N', 'solvers', 'batch', 'nbytes', 'phis', 'ready')
 
     def __init__(self, N, solvers, batch, nbytes, phis):
         self.N = N
@@ -152,12 +153,15 @@ class _Pod:
         self.batch = batch
         self.nbytes = nbytes
         self.phis = phis
+        self.ready = None
 
 
 class PoissonServer:
     """Continuous batching of independent Poisson solves (see the module
     docstring).  slots: requests of one grid size that one launch can carry
-    (1: every request is its own graph launch)."""
+    (1: every request is its own graph launch).  keep_results: True to copy
+    every completed request's potential to `request.phi`, or a function of
+    the request that says whether to keep its potential."""
 
     def __init__(self, h_bohr, nn=3, relax='J', eps=2e-10, precision='fp64',
                  budget_bytes=120 * 2**30, max_inflight=64, nstreams=32, device=None,
@@ -211,6 +215,9 @@ class PoissonServer:
         """Enqueue the requests on the pod's first slots (from phi = 0);
         returns their phis (the pod's buffers)."""
         phis = pod.phis[:len(reqs)]
+        if pod.ready is not None:
+            stream.wait_event(pod.ready)
+            pod.ready = None
         with torch.cuda.stream(stream):
             for phi in phis:
                 phi.zero_()
@@ -285,10 +292,11 @@ class PoissonServer:
         while pending or ninflight or any(queues.values()):
             now = time.perf_counter() - t0
             # retire finished launches
-            for lane in lanes:
+            for li, lane in enumerate(lanes):
                 while lane and lane[0][2].query():
                     pod, reqs, ev, phis = lane.popleft()
                     done = time.perf_counter() - t0
+                    kept = False
                     for slot, (req, phi) in enumerate(zip(reqs, phis)):
                         req.done = done
                         if req.status == 'cancelled':
@@ -298,8 +306,18 @@ class PoissonServer:
                             req.status = 'ok'
                         except Exception as e:  # reported per request
                             req.status = repr(e)
-                        if self.keep_results:
-                            req.phi = phi.clone()
+                        keep = self.keep_results
+                        if keep is not True and callable(keep):
+                            keep = keep(req)
+                        if keep:
+                            # copied on the pod's own stream; the pod's next
+                            # launch (on any stream) waits for the copies
+                            with torch.cuda.stream(self.streams[li]):
+                                req.phi = phi.clone()
+                            kept = True
+                    if kept:
+                        pod.ready = torch.cuda.Event()
+                        pod.ready.record(self.streams[li])
                     ninflight -= 1
                     self.free[pod.N, len(pod.solvers)].append(pod)
                     ev_pool.append(ev)

@@ -376,7 +376,9 @@ typedef struct gfd_tune_plan {
   int form;         /* 0: one thread per point; 1: marching kernel */
   int tile;         /* marching tile: 0 32 columns, 1 16, 2 8, 3 32 columns x 8 rows,
                        4 complex bands with re / im on lane pairs (radius <= 3),
-                       5 the same for complex128 on full rows staged by TMA */
+                       5 the same for complex128 on full rows staged by TMA,
+                       6 complex128, 48 columns x 8 rows (axis-2 lengths that are
+                       multiples of 48) */
   int ctas_per_sm;  /* axis-0 split target */
   double us;        /* measured time per launch, microseconds */
 } gfd_tune_plan;

@@ -227,3 +227,46 @@ def test_autotune_argument_errors(cuda, plans):
     with pytest.raises(NotImplementedError):
         autotune.tune_operator(cross, 1)
     assert autotune.count() == 0
+
+
+@pytest.mark.parametrize('nn', [1, 3, 4])
+@pytest.mark.parametrize('N,pbc', [((12, 20, 96), (1, 1, 1)), ((10, 17, 192), (1, 0, 1)),
+                                   ((9, 24, 97), (0, 1, 0)), ((8, 16, 48), (1, 1, 1))])
+def test_tile48_matches_oracle(cuda, plans, nn, N, pbc):
+    """The 48-column tile (plan tile 6, the built-in choice where axis 2 is
+    a multiple of 48) for complex128 apply and apply with a potential:
+    against the oracle (Bloch phases on every periodic axis, so the wrapped
+    axis-2 halo carries its phase) and bit for bit equal to the short tile
+    (tile 3), which sums in the same order."""
+    import torch
+    from gpaw_b200 import autotune
+    from gpaw_b200.fd_operators import FDOperator
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    og = G.Grid(N, np.array(N) * 0.25, pbc)
+    gd = GridDescriptor(og.N_c, og.cell_cv, og.pbc_c)
+    c, o = G.laplace_stencil(og, -0.5, nn)
+    rng = np.random.default_rng(21 + nn)
+    a = rng.standard_normal((3,) + tuple(og.n_c)) + 1j * rng.standard_normal((3,) + tuple(og.n_c))
+    v = rng.uniform(-1, 1, tuple(og.n_c))
+    ph = G.bloch_phases(og, (0.25, -0.1, 0.3))
+    ref = K.fd_apply(c, o, og.pbc_c, a, ph)
+    t = torch.from_numpy(a).to(cuda)
+    vt = torch.from_numpy(v).to(cuda)
+    op = FDOperator(c, o, gd, t.dtype)
+    res = {}
+    for tile in (6, 3):
+        for mode in (0, 3):
+            force(plans / 'p.txt', 0, 1, mode, og.n_c, nn, per_mask(pbc), 3, (1, tile, 1))
+            got = autotune.operator_plan(op, 3, mode='potential' if mode == 3 else 'apply')
+            assert got is not None and got['tile'] == ('48x8' if tile == 6 else '32x8'), got
+            out = torch.full_like(t, float('nan'))
+            if mode == 0:
+                op.apply(t, out, ph)
+            else:
+                op.apply_with_potential(t, out, vt, ph)
+            torch.cuda.synchronize()
+            res[tile, mode] = out.cpu().numpy()
+            want = ref if mode == 0 else ref + v * a
+            assert rel_err(res[tile, mode], want) < TOL, (tile, mode)
+    for mode in (0, 3):
+        assert np.array_equal(res[6, mode], res[3, mode]), mode

@@ -333,7 +333,9 @@ def test_charged_solve_matches_oracle(cuda, pbc, zero_initial):
     FP64, <= 1e-9 in mixed precision."""
     og = G.Grid((48,) * 3, (48 * 0.2 / BOHR,) * 3, pbc)
     rho = charged_rho(og, 16, 7, 1.0)
-    assert abs(og.integrate(rho) - 1.0) < 1e-3
+    # the zero-boundary grid omits its wall points: the net charge is 1 to
+    # about 2e-3, far above maxcharge (1e-6), so the charged branch runs
+    assert abs(og.integrate(rho) - 1.0) < 1e-2
     rng = np.random.default_rng(3)
     phi0 = 0.01 * rng.standard_normal(tuple(og.n_c))
     phi_o, n_o, _ = solve_oracle(og, rho, phi0=phi0, zero_initial_phi=zero_initial)

@@ -343,10 +343,16 @@ def test_server_metrics_and_cuda_timer(cuda):
     from gpaw_b200.serving import PoissonServer, Request, grid_for, pair_density
     from gpaw_b200.timing import CudaTimer, MetricsLog
     rhos = [pair_density(grid_for(32, H, device=cuda), 70 + i) for i in range(4)]
-    srv = PoissonServer(H, device=cuda, slots=2, nstreams=2)
+    srv = PoissonServer(H, device=cuda, slots=2, nstreams=2,
+                        keep_results=lambda r: r.rid in (1, 2))
     reqs = [Request(i, 32, 0.0, rhos[i]) for i in range(4)]
     buf = io.StringIO()
     stats = srv.run(reqs, metrics=MetricsLog(buf))
+    # only the selected requests' potentials are kept, and they are theirs
+    assert reqs[0].phi is None and reqs[3].phi is None
+    for i in (1, 2):
+        phi, n = solve_alone(cuda, 32, rhos[i])
+        assert reqs[i].niter == n and torch.equal(reqs[i].phi, phi)
     recs = [json.loads(line) for line in buf.getvalue().splitlines()]
     per = [r for r in recs if r['kind'] == 'request']
     assert sorted(r['rid'] for r in per) == [0, 1, 2, 3]

@@ -138,3 +138,59 @@ def test_pseudo_density_interpolation(cuda, pbc):
     assert rel_err(host(out), ref) < TOL
     if not og.pbc_c.all():
         assert abs(of.integrate(host(out)).sum() - pseudo_charge) < 1e-12
+
+
+_RESTRICT_SCRIPT = r'''
+import json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, sys.argv[1] + '/tests')
+import torch
+from oracle import geometry as G
+from oracle import kernels as K
+from conftest import rel_err
+from test_gpu_transfer import gpu_transform, product_grid
+cuda = torch.device('cuda', 0)
+out = []
+for N, pbc in (((24, 16, 40), 1), ((24, 16, 40), 0), ((18, 22, 14), (1, 0, 1)),
+               ((70, 36, 98), 1), ((66, 34, 40), 0)):
+    og = G.Grid(N, np.array(N) * 0.3, pbc)
+    gd = product_grid(og)
+    g2, o2 = gd.coarsen(), og.coarsen()
+    rng = np.random.default_rng(sum(N))
+    a = rng.uniform(-1, 1, (3,) + tuple(og.n_c))
+    ac = a + 1j * rng.uniform(-1, 1, a.shape)
+    ph = G.bloch_phases(og, (0.25, -0.125, 0.3))
+    for nn in (1, 2, 3, 4):
+        try:
+            ref = K.transform(og, o2, nn, a)
+        except AssertionError:
+            continue  # the reference rejects this grid (coarse too small)
+        e64 = rel_err(gpu_transform(cuda, gd, g2, nn, a), ref)
+        e32 = rel_err(gpu_transform(cuda, gd, g2, nn, a, dtype=torch.float32).astype(float), ref)
+        refc = K.transform(og, o2, nn, ac, ph)
+        ec = rel_err(gpu_transform(cuda, gd, g2, nn, ac, ph), refc)
+        ec64 = rel_err(gpu_transform(cuda, gd, g2, nn, ac, ph, dtype=torch.complex64), refc)
+        out.append([list(N), nn, e64, e32, ec, ec64])
+print('RESULT ' + json.dumps(out))
+'''
+
+
+def test_marching_restriction(cuda):
+    """With GFD_DIRECT_MAX=0 every restriction, however small, takes the
+    marching kernel.  Against the oracle for k = 2..8, float64/complex128
+    within 1e-13, float32/complex64 within 2e-6, periodic, zero and mixed
+    boundaries, Bloch phases, tiles cut at every edge."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, GFD_DIRECT_MAX='0')
+    r = subprocess.run([sys.executable, '-c', _RESTRICT_SCRIPT, root], env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    line = [x for x in r.stdout.splitlines() if x.startswith('RESULT ')][-1]
+    for N, nn, e64, e32, ec, ec64 in json.loads(line[len('RESULT '):]):
+        assert e64 < TOL and ec < TOL, (N, nn, e64, ec)
+        assert e32 < 2e-6 and ec64 < 2e-6, (N, nn, e32, ec64)
