@@ -51,6 +51,71 @@ struct StarParams {
   const void* pot;  // MODE_POTENTIAL: real potential v (one grid, type S)
 };
 
+// mbarriers and bounded waits on their phases (the TMA-staged kernels).
+constexpr int kSpinIters = 1 << 26;               // mbarrier wait: iterations
+constexpr long long kSpinCycles = 4000000000LL;   // and SM cycles (about 2 s)
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of the given parity to complete; false when the limit
+// expired first or *abort became nonzero.  test_wait never suspends the
+// thread, so a waiting warp resumes as soon as the phase completes; the
+// iteration count and the cycle counter bound the total time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity,
+                                          const volatile int* abort) {
+  if (mbar_test_wait(b, parity)) return true;
+  const long long t0 = clock64();
+  for (int i = 0; i < kSpinIters; i++) {
+    if (mbar_test_wait(b, parity)) return true;
+    if ((abort && *abort) || clock64() - t0 > kSpinCycles) break;
+  }
+  return false;
+}
+// Bounded wait on an mbarrier phase.  try_wait suspends the thread for a
+// while when the phase is not complete, so waiting warps take few issue
+// slots; the iteration count and the cycle counter bound the total time.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, unsigned parity,
+                                                  const volatile int* abort,
+                                                  long long max_cycles = kSpinCycles) {
+  if (mbar_try_wait(b, parity)) return true;
+  const long long t0 = clock64();
+  for (int i = 0; i < kSpinIters; i++) {
+    if (mbar_try_wait(b, parity)) return true;
+    if ((abort && *abort) || clock64() - t0 > max_cycles) break;
+  }
+  return false;
+}
+
 // Block-wide sum of one double per thread in a fixed order.
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red) {

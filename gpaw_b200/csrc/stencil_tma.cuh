@@ -30,45 +30,6 @@
 namespace gfd {
 
 constexpr int kTmaBZ = 32;                        // columns per CTA
-constexpr int kSpinIters = 1 << 26;               // mbarrier wait: iterations
-constexpr long long kSpinCycles = 4000000000LL;   // and SM cycles (about 2 s)
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_test_wait(uint64_t* b, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Wait for the phase of the given parity to complete; false when the limit
-// expired first or *abort became nonzero.  test_wait never suspends the
-// thread, so a waiting warp resumes as soon as the phase completes; the
-// iteration count and the cycle counter bound the total time.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity,
-                                          const volatile int* abort) {
-  if (mbar_test_wait(b, parity)) return true;
-  const long long t0 = clock64();
-  for (int i = 0; i < kSpinIters; i++) {
-    if (mbar_test_wait(b, parity)) return true;
-    if ((abort && *abort) || clock64() - t0 > kSpinCycles) break;
-  }
-  return false;
-}
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int c0, int c1, int c2, int c3) {
   asm volatile(

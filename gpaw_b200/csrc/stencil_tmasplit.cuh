@@ -110,31 +110,6 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// Bounded wait on an mbarrier phase.  try_wait suspends the thread for a
-// while when the phase is not complete, so waiting warps take few issue
-// slots; the iteration count and the cycle counter bound the total time.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, unsigned parity,
-                                                  const volatile int* abort,
-                                                  long long max_cycles = kSpinCycles) {
-  if (mbar_try_wait(b, parity)) return true;
-  const long long t0 = clock64();
-  for (int i = 0; i < kSpinIters; i++) {
-    if (mbar_try_wait(b, parity)) return true;
-    if ((abort && *abort) || clock64() - t0 > max_cycles) break;
-  }
-  return false;
-}
-
 // One step of the axis-0 ring for ring slot U (= plane index mod Q): add
 // the in-plane part of output plane pl (inp), spread plane pl's own values
 // (own) into the outputs pl - R .. pl + R, and write output pl - R, whose

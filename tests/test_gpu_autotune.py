@@ -236,8 +236,9 @@ def test_tile48_matches_oracle(cuda, plans, nn, N, pbc):
     """The 48-column tile (plan tile 6, the built-in choice where axis 2 is
     a multiple of 48) for complex128 apply and apply with a potential:
     against the oracle (Bloch phases on every periodic axis, so the wrapped
-    axis-2 halo carries its phase) and bit for bit equal to the short tile
-    (tile 3), which sums in the same order."""
+    axis-2 halo carries its phase; zero boundaries on the others) and bit
+    for bit equal to the short tile (tile 3), which sums in the same
+    order."""
     import torch
     from gpaw_b200 import autotune
     from gpaw_b200.fd_operators import FDOperator
@@ -258,7 +259,7 @@ def test_tile48_matches_oracle(cuda, plans, nn, N, pbc):
         for mode in (0, 3):
             force(plans / 'p.txt', 0, 1, mode, og.n_c, nn, per_mask(pbc), 3, (1, tile, 1))
             got = autotune.operator_plan(op, 3, mode='potential' if mode == 3 else 'apply')
-            assert got is not None and got['tile'] == ('48x8' if tile == 6 else '32x8'), got
+            assert got is not None and got['tile'] == {6: '48x8', 3: '32x8'}[tile]
             out = torch.full_like(t, float('nan'))
             if mode == 0:
                 op.apply(t, out, ph)
