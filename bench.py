@@ -603,6 +603,13 @@ def stencil_variants_bench(gd, a, b, phase, steps):
     b32 = torch.empty_like(a32)
     ms = timed(lambda: lap32.apply(a32, b32, phase), steps)
     out['complex64_laplace_GBps'] = 16 * a32.numel() / (ms * 1e-3) / 1e9
+    # the FP32 variant's error against the FP64 apply of the same bands
+    Laplace(gd, -0.5, 3, complex).apply(a, b, phase)
+    err = 0.0
+    for i in range(0, a.shape[0], 64):
+        d = (b32[i:i + 64].to(torch.complex128) - b[i:i + 64]).abs().max().item()
+        err = max(err, d)
+    out['complex64_laplace_max_rel_err_vs_fp64'] = err / b.abs().max().item()
     del a32, b32
     N1 = 48
     gd1 = GridDescriptor((N1,) * 3, (N1 * 0.2 / BOHR,) * 3, 0)

@@ -14,9 +14,11 @@ template <class V, int NN>
 static int restrict_go(const gfd_transformer* tr, const V* in, V* out, int64_t nin,
                        TrParams<typename vt<V>::S>& p, int cps, cudaStream_t s) {
   // Two coarse rows per thread (16 per CTA) stage fewer halo rows per output
-  // row; complex128 keeps one, so two CTAs still fit on an SM.  (28 columns
-  // per CTA, which tile 112 coarse columns exactly, measured slower: 2580
-  // against 2800 GB/s on 256 bands of 112^3.)
+  // row; complex128 keeps one, so two CTAs still fit on an SM.  Other shapes
+  // measured slower on 256 float64 bands of 112^3 (nn = 3; 2800-2830 GB/s
+  // for this one): 28 columns, which tile 112 exactly, 2580; one coarse row
+  // per thread 2270; 32 rows per CTA 2410; 4 rows per thread 2490 (253
+  // registers); three CTAs per SM (80 registers, spills) 1740.
   constexpr int BZC = 32, TYC = 8, VYC = sizeof(V) >= 16 ? 1 : 2, BYC = TYC * VYC;
   constexpr int W = 2 * NN - 1;
   constexpr int RY = 2 * BYC - 1 + 2 * W, RZ = 2 * BZC - 1 + 2 * W;
