@@ -262,7 +262,7 @@ extern "C" int gfd_autotune_operator(gfd_operator* op, int dtype, int mode, cons
     tiles.push_back(TILE_SHORT);
   if (dtype_is_complex(dtype) && op->R <= 3) tiles.push_back(TILE_SPLIT);
   if (dtype == GFD_COMPLEX128 && op->R <= 3) tiles.push_back(TILE_TMASPLIT);
-  if (dtype == GFD_COMPLEX128 && (imode == OP_APPLY || imode == OP_POTENTIAL) &&
+  if (dtype_is_complex(dtype) && (imode == OP_APPLY || imode == OP_POTENTIAL) &&
       tile48_eligible(op))
     tiles.push_back(TILE_48);
   const std::vector<TunePlan> cands = march_candidates(tiles);

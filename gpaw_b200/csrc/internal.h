@@ -60,7 +60,7 @@ int num_sms();
 // pairs (star_split_kernel): 32 columns by 16 rows, 128 threads.
 // TILE_TMASPLIT: complex128, radius <= 3, the same lane pairs on full-row
 // tiles of 8 rows staged by TMA (star_tmasplit_kernel).
-// TILE_48: complex128 apply (and apply with a potential) up to radius 4,
+// TILE_48: complex apply (and apply with a potential) up to radius 4,
 // 48 columns by 8 rows (48 x 4 threads, 2 rows each, two CTAs per SM), for
 // axis-2 lengths that are multiples of 48: it stages 2R halo columns per 48
 // where the 32-column tiles stage 2R per 32.

@@ -271,3 +271,16 @@ def test_tile48_matches_oracle(cuda, plans, nn, N, pbc):
             assert rel_err(res[tile, mode], want) < TOL, (tile, mode)
     for mode in (0, 3):
         assert np.array_equal(res[6, mode], res[3, mode]), mode
+    # complex64 bands: the 48-column tile (now built-in there) against the
+    # 32 x 16 tile (plan tile 0, same summation order) and the FP64 oracle
+    t64 = t.to(torch.complex64)
+    op64 = FDOperator(c, o, gd, t64.dtype)
+    r64 = {}
+    for tile in (6, 0):
+        force(plans / 'p.txt', 0, 3, 0, og.n_c, nn, per_mask(pbc), 3, (1, tile, 1))
+        out = torch.full_like(t64, float('nan'))
+        op64.apply(t64, out, ph)
+        torch.cuda.synchronize()
+        r64[tile] = out.cpu().numpy()
+    assert np.array_equal(r64[6], r64[0])
+    assert rel_err(r64[6].astype(complex), ref) < 2e-6
